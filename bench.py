@@ -1,0 +1,379 @@
+"""Benchmark: neighbour-list pairs/s on B200 for the dense-bulk configuration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one "step" = one full neighbour_list("ijdDS") build): 1,048,576 atoms
+on an FCC lattice (a = 3.6 A, 64^3 unit cells), Gaussian jitter 0.1 A, cell
+sheared by xy = 0.2 Lx and xz = 0.1 Lx, periodic, cutoff 5.0 A, FP64 -- seeded
+synthetic data.  Each step bins, sorts, counts, scans and fills the exact pair
+list (bit-identical to the reference CPU path).
+
+* value: pairs/s with positions resident in HBM, device time per step from
+  CUDA events on the engine's stream, L2 flushed (a 256 MiB write) between
+  steps outside the timed events; whole-job aggregate over ranks.
+* e2e:   the same metric through the public API with host numpy buffers:
+  every step copies the positions host->device and all five output arrays
+  device->host (pinned host memory).
+* roofline: the fill kernel (the HBM-bound pass that writes 52 B per pair),
+  algorithmic bytes (npairs * 52 + nat * 24) / its CUDA-event time, against
+  the measured HBM copy bandwidth.
+* cpu_baseline: the reference's own CPU core (oracle/_ref, OpenMP, all host
+  threads) on the same workload, rank 0 at N = 1.
+
+Under torchrun each rank builds its own replica of the workload (seed = rank):
+independent systems, no collective on the data path (weak scaling).
+"""
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "matscipy-neighbours_b200"))
+
+WORKLOAD = {"workload": "fcc_bulk_triclinic_1M", "natoms": 1048576, "lattice": "fcc",
+            "a_A": 3.6, "reps": 64, "jitter_A": 0.1, "shear": [0.2, 0.1],
+            "pbc": "TTT", "cutoff_A": 5.0, "quantities": "ijdDS"}
+METRIC = "pairs/s (exact pair set, dense bulk FCC 1M atoms, ijdDS)"
+UNIT = "pairs/s"
+BYTES_PER_PAIR = 52   # i 4 + j 4 + d 8 + D 24 + S 12
+BYTES_PER_ATOM_IN = 24
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured", d
+        except Exception:
+            pass
+    return 6650.0, "fallback", {}
+
+
+def _traffic_per_launch(npairs, nat):
+    p = ROOT / "profiles" / "fill_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d["bytes_per_pair"] * npairs + d.get("bytes_per_atom", 0.0) * nat
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names[1:], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps=2):
+    """The reference's CPU core on the same workload (rank 0, N = 1)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from matscipy_neighbours import _workloads as W
+    w = W.fcc_bulk(seed=0)
+    cores = len(os.sched_getaffinity(0))
+    if O.ref_available():
+        kind = "reference"
+        O.ref_set_threads(cores)
+        fn = O.ref_neighbour_list
+    else:
+        kind, cores = "port", 1
+        fn = O.oracle_neighbour_list
+    fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])  # warm-up
+    times, npairs = [], 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        i = fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])[0]
+        times.append(time.perf_counter() - t0)
+        npairs = len(i)
+    med = statistics.median(times)
+    return {"value": npairs / med, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"full workload ({npairs} pairs), median of {steps} calls",
+            "seconds_per_call": med}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from matscipy_neighbours import _workloads as W
+    w = W.fcc_bulk(seed=0)
+    cores = len(os.sched_getaffinity(0))
+    if O.ref_available():
+        kind = "reference"
+        O.ref_set_threads(cores)
+        fn = O.ref_neighbour_list
+    else:
+        kind, cores = "port", 1
+        fn = O.oracle_neighbour_list
+    for _ in range(args.warmup):
+        fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])
+    times, npairs = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        npairs = len(fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])[0])
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = npairs * args.steps / total
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="host threads"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"full workload ({npairs} pairs) per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import matscipy_neighbours as m
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    from matscipy_neighbours import _workloads as W
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    w = W.fcc_bulk(seed=rank)
+    nat = w["positions"].shape[0]
+    cell = np.ascontiguousarray(w["cell"])
+    inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+    origin = np.zeros(3)
+    pbc8 = np.ones(3, dtype=np.uint8)
+    pos_d = torch.from_numpy(w["positions"]).to(dev)
+    stream = torch.cuda.Stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    plan = ext.plan_for(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def request(precision):
+        prev = ext.set_options(precision=precision, grid="auto")
+        r = ext.make_request(31, origin, cell, inv, pbc8, nat,
+                             ctypes.c_void_p(pos_d.data_ptr()), True, w["cutoff"], None,
+                             None, 0, None, local)
+        ext.set_options(**{"precision": prev["precision"], "grid": prev["grid"]})
+        return r
+
+    npairs_c = ctypes.c_int64()
+    req = request("fp32")
+    with torch.cuda.stream(stream):
+        ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(npairs_c)))
+    npairs = int(npairs_c.value)
+    outs = {"i": torch.empty(npairs, dtype=torch.int32, device=dev),
+            "j": torch.empty(npairs, dtype=torch.int32, device=dev),
+            "D": torch.empty((npairs, 3), dtype=torch.float64, device=dev),
+            "d": torch.empty(npairs, dtype=torch.float64, device=dev),
+            "S": torch.empty((npairs, 3), dtype=torch.int32, device=dev)}
+    ostruct = ext._outputs_struct(outs, lambda t: t.data_ptr())
+
+    def timed_steps(req, k, record=True):
+        """k full builds; returns (per-step ms, per-fill ms)."""
+        step_ms, fill_ms = [], []
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e2 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr,
+                                        ctypes.byref(npairs_c)))
+            e1.record(stream)
+            ext.check(ext.lib.nbl_fill(plan, ctypes.byref(ostruct), sptr))
+            e2.record(stream)
+            e2.synchronize()
+            step_ms.append(e0.elapsed_time(e2))
+            fill_ms.append(e1.elapsed_time(e2))
+        return step_ms, fill_ms
+
+    # --- FP32-filter path (the headline), then plain FP64 for comparison ----
+    timed_steps(req, args.warmup)
+    ext.check(ext.lib.nbl_check(plan, sptr))
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ext.lib.nbl_launch_count(1)
+    step_ms, fill_ms = timed_steps(req, args.steps)
+    launches = int(ext.lib.nbl_launch_count(1))
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    ext.check(ext.lib.nbl_check(plan, sptr))
+
+    req64 = request("fp64")
+    timed_steps(req64, 2)
+    step64, fill64 = timed_steps(req64, max(3, args.steps // 2))
+
+    total_ms = sum(step_ms)
+    pairs_job = npairs * args.steps
+    if dist is not None:
+        t = torch.tensor([total_ms, float(pairs_job)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms, pairs_job = float(tmax[0]), float(t[1])
+    value = pairs_job / (total_ms * 1e-3)
+
+    # --- end to end through the public API with host buffers ----------------
+    host_pos = ext.host_empty((nat, 3), np.float64)
+    host_pos[...] = w["positions"]
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = m.neighbour_list("ijdDS", positions=host_pos, cell=cell, pbc=w["pbc"],
+                               cutoff=w["cutoff"])
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_times.append(t1 - t0)
+        del res
+    e2e_total = sum(e2e_times)
+    e2e_pairs = npairs * len(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_total, float(e2e_pairs)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        e2e_total, e2e_pairs = float(tmax[0]), float(t[1])
+    e2e_value = e2e_pairs / e2e_total
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind, peaks = _peaks()
+    fill_avg_s = statistics.mean(fill_ms) * 1e-3
+    alg_bytes = npairs * BYTES_PER_PAIR + nat * BYTES_PER_ATOM_IN
+    achieved = alg_bytes / fill_avg_s / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, npairs_per_step=npairs, parallelism=f"replicas{world}",
+                       l2="flushed between steps (256 MiB write, outside the events)",
+                       precision="fp32 filter + fp64 guard-band recheck"),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": _traffic_per_launch(npairs, nat),
+                     "kernel": "k_traverse<FILL> (fill pass)",
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "fill_ms": statistics.mean(fill_ms)},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": nat * 3 * 8,
+                "d2h_bytes_per_step": npairs * BYTES_PER_PAIR,
+                "ms_per_step": 1e3 * statistics.mean(e2e_times)},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "fp64_plain": {"value": npairs / (statistics.mean(step64) * 1e-3),
+                       "ms_per_step": statistics.mean(step64),
+                       "fill_ms": statistics.mean(fill64)},
+        "stage_ms": {"count_phase": statistics.mean(a - b for a, b in zip(step_ms, fill_ms)),
+                     "fill": statistics.mean(fill_ms)},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/*
+ * nbl_b200.h -- C-ABI of the B200 neighbour-list engine.
+ *
+ * The engine is a drop-in for the device path of matscipy-neighbours'
+ * `neighbour_list(quantities, positions, cell, pbc, cutoff)`.  Every entry
+ * point takes plain pointers and sizes, returns an nbl_status and never aborts
+ * the process; on failure a thread-local message is available from
+ * nbl_last_error().  No torch (or other framework) type appears here.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - NeighbourListRequest           src/libneighbours/neighbour_list_gpu.hh:49-65
+ *       -> nbl_request
+ *   - neighbour_list_gpu_device()    src/libneighbours/neighbour_list_gpu.hh:95-96
+ *       -> nbl_neighbour_list_device() (and the two-phase nbl_count/nbl_fill)
+ *   - neighbour_count_gpu_device()   src/libneighbours/neighbour_list_gpu.hh:101-102
+ *       -> nbl_count + nbl_counts
+ *   - neighbour_list_gpu() (host in, host out)
+ *                                    src/libneighbours/neighbour_list_gpu.hh:28-34
+ *       -> nbl_count + nbl_fill_host (host positions, host outputs)
+ *   - error_t / has_error / error_string
+ *                                    src/libneighbours/types.hh:32-34,
+ *                                    src/libneighbours/error.hh:27-33
+ *       -> nbl_status + nbl_last_error()
+ *   - Quantity flags                 src/libneighbours/types.hh:38-44
+ *       -> NBL_QUANTITY_* (same bit values)
+ *   - _has_gpu / _device_type        language_bindings/python/module.c:104-113
+ *       -> nbl_has_gpu() / nbl_device_type()
+ *
+ * Output contract (identical to the reference CPU path, neighbour_list.cc:
+ * 40-95): pairs sorted by i, and within one i in the reference's traversal
+ * order; D (npairs x 3, row-major) satisfies D == r[j] - r[i] + S @ cell;
+ * d = |D| correctly rounded; i, j, S are int32; D, d are float64.
+ */
+#ifndef NBL_B200_H
+#define NBL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NBL_API __attribute__((visibility("default")))
+#else
+#define NBL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum nbl_status {
+    NBL_SUCCESS = 0,
+    NBL_ERROR_INVALID_ARGUMENT = 1, /* bad sizes / pointers / flags          */
+    NBL_ERROR_ZERO_VOLUME = 2,      /* "Zero cell volume." (cell_list.cc:161) */
+    NBL_ERROR_RANGE = 3,            /* non-finite position, or an atom more
+                                       than 2^29 cells outside the box        */
+    NBL_ERROR_OUT_OF_MEMORY = 4,
+    NBL_ERROR_CUDA = 5,             /* a CUDA runtime error (message says which) */
+    NBL_ERROR_CAPACITY = 6,         /* output capacity smaller than the pair
+                                       count (batched / graph path); retry     */
+    NBL_ERROR_NO_DEVICE = 7,
+    NBL_ERROR_INTERNAL = 8          /* a device-side bound was hit (never
+                                       expected; reported instead of hanging)  */
+} nbl_status;
+
+/* Quantity bits, same values as matscipy::Quantity (types.hh:38-44). */
+#define NBL_QUANTITY_FIRST 1   /* i */
+#define NBL_QUANTITY_SECOND 2  /* j */
+#define NBL_QUANTITY_DISTVEC 4 /* D */
+#define NBL_QUANTITY_ABSDIST 8 /* d */
+#define NBL_QUANTITY_SHIFT 16  /* S */
+
+/* Cell grid layout.  All produce identical output; they differ in memory
+   layout and lookup only (the reference's CellOrder Linear/Morton,
+   cell_list.hh:25, and its dense/sparse backends, cell_list.cc:184-203). */
+typedef enum nbl_grid {
+    NBL_GRID_AUTO = 0,   /* dense, or hashed when the grid is far larger than
+                            the atom count (the reference's own rule)      */
+    NBL_GRID_DENSE = 1,  /* dense table, cells in linear (z-major) order   */
+    NBL_GRID_MORTON = 2, /* dense table, atoms laid out in Morton order    */
+    NBL_GRID_HASHED = 3  /* hashed compact table of occupied cells only    */
+} nbl_grid;
+
+/* Candidate-test precision.  Both give the reference's exact pair set and
+   bit-identical D and d; FP32_FILTER rejects most candidates in FP32 and
+   re-tests only those inside a rigorous guard band of the cutoff in FP64. */
+typedef enum nbl_precision {
+    NBL_PRECISION_FP32_FILTER = 0,
+    NBL_PRECISION_FP64 = 1
+} nbl_precision;
+
+/* One system.  Mirrors NeighbourListRequest (neighbour_list_gpu.hh:49-65).
+   Geometry arrays are host memory.  `pbc` entries are 0/1 bytes. */
+typedef struct nbl_request {
+    int quantities;                    /* NBL_QUANTITY_* bits                 */
+    const double *cell_origin;         /* [3]                                 */
+    const double *cell;                /* [9] row-major, rows = lattice vectors */
+    const double *inv_cell;            /* [9] inv(cell.T): inv_cell . r = frac */
+    const uint8_t *pbc;                /* [3]                                 */
+    int64_t nat;
+    const double *positions;           /* [3*nat] row-major                   */
+    int positions_on_device;           /* 1: device pointer, used in place    */
+    double cutoff;                     /* binning / global cutoff             */
+    const double *per_atom_cutoff;     /* [nat] radii (pair cutoff = sum) or NULL */
+    const double *per_type_cutoff_sq;  /* [ncutoffs^2] host, squared, or NULL */
+    int32_t ncutoffs;
+    const int32_t *types;              /* [nat] or NULL                       */
+    int aux_on_device;                 /* per_atom_cutoff / types on device   */
+    int grid;                          /* nbl_grid                            */
+    int precision;                     /* nbl_precision                       */
+    int device_id;                     /* -1: current device                  */
+} nbl_request;
+
+/* Output buffers for one fill.  NULL skips a quantity.  Device pointers for
+   nbl_fill, host pointers for nbl_fill_host.  Each must hold npairs entries
+   (distvec and shift 3*npairs). */
+typedef struct nbl_outputs {
+    int32_t *first;
+    int32_t *second;
+    double *distvec;
+    double *absdist;
+    int32_t *shift;
+} nbl_outputs;
+
+/* Opaque state: device workspace reused across calls, plus the result of the
+   last count phase.  A plan belongs to one device; calls on one plan must not
+   overlap (use one plan per host thread). */
+typedef struct nbl_plan nbl_plan;
+
+NBL_API nbl_status nbl_plan_create(int device_id, nbl_plan **plan);
+NBL_API nbl_status nbl_plan_destroy(nbl_plan *plan);
+/* Releases the plan's device workspace (it is re-grown on the next call). */
+NBL_API nbl_status nbl_plan_trim(nbl_plan *plan);
+
+/* Count phase: bins the atoms, counts every atom's neighbours and scans the
+   counts into row offsets.  Host positions are copied in on `stream`.
+   Synchronises `stream` to return the pair count. */
+NBL_API nbl_status nbl_count(nbl_plan *plan, const nbl_request *req, void *stream,
+                     int64_t *npairs);
+
+/* Fill phase for the last nbl_count: writes the requested quantities into
+   caller-allocated device buffers, asynchronously on `stream`. */
+NBL_API nbl_status nbl_fill(nbl_plan *plan, const nbl_outputs *out, void *stream);
+
+/* Fill into HOST buffers: fills device scratch owned by the plan and copies
+   each requested quantity back; returns after the copies complete. */
+NBL_API nbl_status nbl_fill_host(nbl_plan *plan, const nbl_outputs *host_out,
+                         void *stream);
+
+/* Synchronises `stream` and reports any error the device flagged during the
+   last count/fill (capacity overflow, internal bound); NBL_SUCCESS if none. */
+NBL_API nbl_status nbl_check(nbl_plan *plan, void *stream);
+
+/* Per-atom neighbour counts (coordination numbers, original atom order) of
+   the last nbl_count, into a device int32[nat] buffer, on `stream`.
+   (neighbour_count_gpu_device, neighbour_list_gpu.hh:101-102.) */
+NBL_API nbl_status nbl_counts(nbl_plan *plan, int32_t *counts, void *stream);
+
+/* Dense fixed-capacity neighbour matrix of the last nbl_count
+   (neighbour_matrix_gpu_device, neighbour_list_gpu.hh:112-123): row a of the
+   device buffers idx [nat*K] int32 and dist [nat*K*3] float64 holds atom a's
+   first min(count[a], K) neighbours (j and D) in the reference's row order;
+   unused slots are 0; count [nat] int32 holds the full degree.  *overflow
+   (host int) is set to 1 when some atom has more than K neighbours.
+   Synchronises `stream`. */
+NBL_API nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours,
+                                   int32_t *idx, double *dist, int32_t *count,
+                                   int *overflow, void *stream);
+
+/* Row offsets (exclusive prefix of the counts, int64[nat+1], device) of the
+   last nbl_count, on `stream`: row i of the pair list is [off[i], off[i+1]). */
+NBL_API nbl_status nbl_row_offsets(nbl_plan *plan, int64_t *offsets, void *stream);
+
+/* One-shot device entry (neighbour_list_gpu_device): the library allocates
+   the outputs with stream-ordered allocation on `stream`; release them with
+   nbl_device_result_free on a stream ordered after their last use. */
+typedef struct nbl_device_result {
+    int64_t npairs;
+    int32_t *first;
+    int32_t *second;
+    double *distvec;
+    double *absdist;
+    int32_t *shift;
+    int device_id;
+} nbl_device_result;
+
+NBL_API nbl_status nbl_neighbour_list_device(const nbl_request *req, void *stream,
+                                     nbl_device_result *result);
+NBL_API nbl_status nbl_device_result_free(nbl_device_result *result, void *stream);
+
+/* Last error message of the calling thread ("" if none). */
+NBL_API const char *nbl_last_error(void);
+
+/* Number of CUDA kernels this library launched from the calling thread since
+   the last reset (reset when `reset` is non-zero). */
+NBL_API long long nbl_launch_count(int reset);
+
+/* 1 if a CUDA device is visible, else 0 (module.c:104-113 `_has_gpu`). */
+NBL_API int nbl_has_gpu(void);
+/* DLPack device type of the outputs: 2 (kDLCUDA). */
+NBL_API int nbl_device_type(void);
+/* Library version string. */
+NBL_API const char *nbl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NBL_B200_H */

@@ -1,0 +1,882 @@
+// nbl_api.cu -- host side of the engine: request validation, bit-exact grid
+// planning, workspace management and the C-ABI of include/nbl_b200.h.
+//
+// Host arithmetic that feeds the kernels (cell widths, cells per direction,
+// bin vectors, scan ranges, cutoff^2) follows the reference's operation order
+// (src/libneighbours/cell_list.cc:153-182, neighbour_list.cc:169-192) and is
+// compiled without FP contraction, so the device sees the same doubles the
+// reference CPU core computes.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "nbl_b200.h"
+#include "nbl_build.cuh"
+#include "nbl_internal.cuh"
+#include "nbl_plan.hh"
+#include "nbl_sort.cuh"
+
+namespace nbl {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+nbl_status set_error(nbl_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+static void clear_error() { g_last_error.clear(); }
+
+static thread_local long long g_launches = 0;
+void count_launch(int n) { g_launches += n; }
+
+nbl_status cuda_status(cudaError_t e, const char *where) {
+    if (e == cudaSuccess) return NBL_SUCCESS;
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(NBL_ERROR_OUT_OF_MEMORY, "%s: out of device memory", where);
+    return set_error(NBL_ERROR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define NBL_CUDA(call, where)                                  \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_status(e_, where);  \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// geometry (cell_list.cc:153-182 and neighbour_list.cc:169-192)
+// ---------------------------------------------------------------------------
+
+// static_cast<int>(double) as x86-64 executes it: out of range or NaN gives
+// INT32_MIN (cvttsd2si).  The reference relies on it for very small cutoffs
+// (len/cutoff beyond 2^31 gives n = max(INT32_MIN, 1) = 1).
+static int32_t x86_to_i32(double v) {
+    if (!(v > -2147483649.0 && v < 2147483648.0)) return INT32_MIN;
+    return (int32_t)v;
+}
+
+static void cross3(const double *a, const double *b, double *c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static double norm3(const double *a) {
+    return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+}
+
+nbl_status plan_system(const double origin[3], const double cell[9],
+                       const double inv_cell[9], const uint8_t pbc[3],
+                       double cutoff, SysDev &S, int64_t &ncells) {
+    std::memset(&S, 0, sizeof(S));
+    if (!std::isfinite(cutoff))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "cutoff must be finite");
+    const double *c1 = &cell[0], *c2 = &cell[3], *c3 = &cell[6];
+    double nrm1[3], nrm2[3], nrm3[3];
+    cross3(c2, c3, nrm1);
+    cross3(c3, c1, nrm2);
+    cross3(c1, c2, nrm3);
+    const double volume =
+        std::fabs(c3[0] * nrm3[0] + c3[1] * nrm3[1] + c3[2] * nrm3[2]);
+    if (volume < 1e-12) return set_error(NBL_ERROR_ZERO_VOLUME, "Zero cell volume.");
+    double len[3];
+    len[0] = volume / norm3(nrm1);
+    len[1] = volume / norm3(nrm2);
+    len[2] = volume / norm3(nrm3);
+    for (int k = 0; k < 3; k++) {
+        const int32_t n = x86_to_i32(std::floor(len[k] / cutoff));
+        S.n[k] = std::max(n, 1);
+    }
+    for (int k = 0; k < 3; k++) {
+        S.bin[0][k] = c1[k] / S.n[0];
+        S.bin[1][k] = c2[k] / S.n[1];
+        S.bin[2][k] = c3[k] / S.n[2];
+        S.origin[k] = origin[k];
+        S.pbc[k] = pbc[k] ? 1 : 0;
+    }
+    for (int k = 0; k < 9; k++) S.inv[k] = inv_cell[k];
+    int64_t nvisit = 1;
+    for (int k = 0; k < 3; k++) {
+        const double s = cutoff * S.n[k] / len[k];
+        const double cs = std::ceil(s);
+        if (!(cs < 1e6))
+            return set_error(NBL_ERROR_INVALID_ARGUMENT,
+                             "cutoff spans more than 10^6 periodic images of the cell");
+        S.nscan[k] = (int32_t)cs;
+        nvisit *= (S.nscan[k] < 0) ? 0 : (2 * (int64_t)S.nscan[k] + 1);
+    }
+    if (nvisit > (int64_t(1) << 24))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT,
+                         "cutoff spans more than 2^24 neighbour cells per cell");
+    S.nvisit = (int32_t)nvisit;
+    S.cutoff = cutoff;
+    S.cutoff_sq = cutoff * cutoff;
+    double off_max = 0.0;
+    for (int k = 0; k < 3; k++) {
+        const double bmax = std::max(std::fabs(S.bin[k][0]),
+                                     std::max(std::fabs(S.bin[k][1]), std::fabs(S.bin[k][2])));
+        off_max += std::max(S.nscan[k], 0) * bmax;
+    }
+    S.off_max = off_max * (1.0 + 1e-12);
+    ncells = (int64_t)S.n[0] * S.n[1] * S.n[2];
+    return NBL_SUCCESS;
+}
+
+static int bits_for(uint64_t maxval) {
+    int b = 0;
+    while (b < 64 && (maxval >> b) != 0) b++;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// workspace
+// ---------------------------------------------------------------------------
+
+struct Layout {
+    size_t total = 0;
+    size_t add(size_t bytes) {
+        size_t off = total;
+        total += (bytes + 255) & ~size_t(255);
+        return off;
+    }
+};
+
+void Workspace::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    bytes = 0;
+    if (out_base) cudaFree(out_base);
+    out_base = nullptr;
+    out_bytes = 0;
+}
+
+static nbl_status ensure(void *&ptr, size_t &have, size_t need, const char *what) {
+    if (need <= have) return NBL_SUCCESS;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    have = 0;
+    size_t grow = need + need / 4;
+    cudaError_t e = cudaMalloc(&ptr, grow);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&ptr, need);
+        grow = need;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return set_error(NBL_ERROR_OUT_OF_MEMORY, "%s: cannot allocate %zu bytes", what,
+                         need);
+    }
+    have = grow;
+    return NBL_SUCCESS;
+}
+
+// Carve the per-call buffers out of the plan's workspace.
+static nbl_status layout_workspace(Plan &p, const Batch &b) {
+    const int64_t N = b.natoms;
+    const int64_t nsys = (int64_t)b.sys.size();
+    const int64_t hist = radix_hist_elems(std::max<int64_t>(N, 1));
+    Layout L;
+    Bufs &B = p.bufs;
+    size_t o_pos = b.pos_on_device ? 0 : L.add(sizeof(double) * 3 * N);
+    size_t o_pa = (b.per_atom && !b.aux_on_device) ? L.add(sizeof(double) * N) : 0;
+    size_t o_ty = (b.types && !b.aux_on_device) ? L.add(sizeof(int32_t) * N) : 0;
+    size_t o_sys = L.add(sizeof(SysDev) * nsys);
+    size_t o_sab = L.add(sizeof(int64_t) * nsys);
+    size_t o_pt64 = L.add(sizeof(double) * std::max<size_t>(b.pt64.size(), 1));
+    size_t o_pt32 = L.add(sizeof(float) * std::max<size_t>(b.pt64.size(), 1));
+    size_t o_keys = L.add(sizeof(uint32_t) * N);
+    size_t o_vals = L.add(sizeof(int32_t) * N);
+    size_t o_keys2 = L.add(sizeof(uint32_t) * N);
+    size_t o_vals2 = L.add(sizeof(int32_t) * N);
+    size_t o_hist = L.add(sizeof(int32_t) * hist);
+    size_t o_hscan = L.add(sizeof(int32_t) * hist);
+    size_t o_sscr32 = L.add(sizeof(int32_t) * scan_scratch_elems(hist));
+    size_t o_sscr64 = L.add(sizeof(int64_t) * scan_scratch_elems(N + 1));
+    size_t o_table = L.add(sizeof(int2) * b.table_size);
+    size_t o_hkey = b.grid == kGridHashed ? L.add(sizeof(unsigned long long) * b.table_size) : 0;
+    size_t o_pos64 = L.add(sizeof(double4) * N);
+    size_t o_pos32 = L.add(sizeof(float4) * N);
+    size_t o_aux = L.add(sizeof(int4) * N);
+    size_t o_amax = L.add(sizeof(float) * nsys);
+    size_t o_home = L.add(sizeof(HomeCell) * N);
+    size_t o_cnt = L.add(sizeof(int32_t) * (N + 1));
+    size_t o_off = L.add(sizeof(int64_t) * (N + 1));
+    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err
+    nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
+    if (st != NBL_SUCCESS) return st;
+    char *base = static_cast<char *>(p.ws.base);
+    auto at = [&](size_t off) { return static_cast<void *>(base + off); };
+    B.pos = b.pos_on_device ? const_cast<double *>(b.positions) : (double *)at(o_pos);
+    B.per_atom = b.per_atom ? (b.aux_on_device ? const_cast<double *>(b.per_atom)
+                                               : (double *)at(o_pa))
+                            : nullptr;
+    B.types = b.types ? (b.aux_on_device ? const_cast<int32_t *>(b.types)
+                                         : (int32_t *)at(o_ty))
+                      : nullptr;
+    B.sys = (SysDev *)at(o_sys);
+    B.sys_atom_base = (int64_t *)at(o_sab);
+    B.pt64 = (double *)at(o_pt64);
+    B.pt32 = (float *)at(o_pt32);
+    B.keys = (uint32_t *)at(o_keys);
+    B.vals = (int32_t *)at(o_vals);
+    B.keys2 = (uint32_t *)at(o_keys2);
+    B.vals2 = (int32_t *)at(o_vals2);
+    B.hist = (int32_t *)at(o_hist);
+    B.hist_scan = (int32_t *)at(o_hscan);
+    B.scan32 = (int32_t *)at(o_sscr32);
+    B.scan64 = (int64_t *)at(o_sscr64);
+    B.table = (int2 *)at(o_table);
+    B.hkey = b.grid == kGridHashed ? (unsigned long long *)at(o_hkey) : nullptr;
+    B.pos64 = (double4 *)at(o_pos64);
+    B.pos32 = (float4 *)at(o_pos32);
+    B.aux = (int4 *)at(o_aux);
+    B.amax = (float *)at(o_amax);
+    B.home = (HomeCell *)at(o_home);
+    B.counts = (int32_t *)at(o_cnt);
+    B.offsets = (int64_t *)at(o_off);
+    B.small = (int *)at(o_small);
+    return NBL_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// batch planning
+// ---------------------------------------------------------------------------
+
+nbl_status finish_batch(Batch &b, int grid_req) {
+    const int64_t nsys = (int64_t)b.sys.size();
+    if (b.natoms > INT32_MAX - 1)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "more than 2^31-2 atoms");
+    int64_t total_cells = 0, total_morton = 0;
+    bool morton_ok = true;
+    for (int64_t s = 0; s < nsys; s++) {
+        const SysDev &S = b.sys[s];
+        total_cells += b.ncells[s];
+        const int32_t nmax = std::max(S.n[0], std::max(S.n[1], S.n[2]));
+        if (nmax > 1024) morton_ok = false;
+        const int mb = bits_for((uint64_t)(nmax - 1));
+        total_morton += int64_t(1) << (3 * mb);
+        if (b.ncells[s] >= (int64_t(1) << kHashSysShift))
+            return set_error(NBL_ERROR_INVALID_ARGUMENT, "cell grid too large");
+    }
+    if (nsys >= (int64_t(1) << (64 - kHashSysShift - 1)))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "too many systems");
+    const int64_t budget = std::max<int64_t>(int64_t(1) << 20, 8 * b.natoms);
+    int grid = grid_req;
+    if (grid == NBL_GRID_AUTO) grid = total_cells > budget ? NBL_GRID_HASHED : NBL_GRID_DENSE;
+    if ((grid == NBL_GRID_DENSE || grid == NBL_GRID_MORTON) &&
+        total_cells > (int64_t(1) << 31) - 2)
+        grid = NBL_GRID_HASHED;
+    if (grid == NBL_GRID_MORTON && (!morton_ok || total_morton > (int64_t(1) << 32) - 2))
+        grid = NBL_GRID_DENSE;
+    b.grid = grid == NBL_GRID_HASHED ? kGridHashed
+             : (grid == NBL_GRID_MORTON ? kGridMorton : kGridDense);
+    int64_t cell_base = 0, key_base = 0;
+    for (int64_t s = 0; s < nsys; s++) {
+        SysDev &S = b.sys[s];
+        S.cell_base = cell_base;
+        S.key_base = (b.grid == kGridMorton) ? key_base : cell_base;
+        cell_base += b.ncells[s];
+        const int32_t nmax = std::max(S.n[0], std::max(S.n[1], S.n[2]));
+        key_base += int64_t(1) << (3 * bits_for((uint64_t)(nmax - 1)));
+    }
+    if (b.grid == kGridHashed) {
+        int64_t cap = 1;
+        while (cap < 2 * std::max<int64_t>(b.natoms, 1) + 1) cap <<= 1;
+        b.table_size = cap;
+        b.key_bits = bits_for((uint64_t)(cap - 1));
+    } else {
+        b.table_size = std::max<int64_t>(total_cells, 1);
+        b.key_bits = b.grid == kGridMorton ? bits_for((uint64_t)(key_base - 1))
+                                           : bits_for((uint64_t)(total_cells - 1));
+    }
+    return NBL_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// count / fill
+// ---------------------------------------------------------------------------
+
+static int traverse_grid(const Plan &p, int64_t natoms) {
+    // Persistent-style grid: a few resident CTAs per SM, capped by the number
+    // of possible home cells.
+    const int64_t g = std::min<int64_t>((int64_t)p.num_sms * 6, std::max<int64_t>(natoms, 1));
+    return (int)g;
+}
+
+nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
+    nbl_status s = layout_workspace(p, b);
+    if (s != NBL_SUCCESS) return s;
+    Bufs &B = p.bufs;
+    const int64_t N = b.natoms;
+    const int nsys = (int)b.sys.size();
+    p.batch_natoms = N;
+    p.batch_nsys = nsys;
+    p.batch_fp32 = b.fp32;
+    p.batch_grid = b.grid;
+    p.have_count = false;
+
+    if (!b.pos_on_device && N > 0)
+        NBL_CUDA(cudaMemcpyAsync(B.pos, b.positions, sizeof(double) * 3 * N,
+                                 cudaMemcpyHostToDevice, st), "copy positions");
+    if (b.per_atom && !b.aux_on_device && N > 0)
+        NBL_CUDA(cudaMemcpyAsync(B.per_atom, b.per_atom, sizeof(double) * N,
+                                 cudaMemcpyHostToDevice, st), "copy per-atom cutoffs");
+    if (b.types && !b.aux_on_device && N > 0)
+        NBL_CUDA(cudaMemcpyAsync(B.types, b.types, sizeof(int32_t) * N,
+                                 cudaMemcpyHostToDevice, st), "copy types");
+    // Small host tables go through the plan's pinned staging so the copies
+    // are truly asynchronous and the staging stays valid until they run.
+    {
+        size_t need = sizeof(SysDev) * nsys + sizeof(int64_t) * nsys +
+                      (sizeof(double) + sizeof(float)) * b.pt64.size() + 64;
+        if (need > p.host_stage_bytes) {
+            if (p.host_stage) {
+                cudaStreamSynchronize(st);
+                cudaFreeHost(p.host_stage);
+            }
+            p.host_stage = nullptr;
+            p.host_stage_bytes = 0;
+            NBL_CUDA(cudaMallocHost(&p.host_stage, need * 2), "pinned staging");
+            p.host_stage_bytes = need * 2;
+        } else if (p.stage_in_flight) {
+            // The previous call's staging copies must have run before reuse.
+            NBL_CUDA(cudaEventSynchronize(p.stage_done), "staging reuse");
+        }
+        char *h = static_cast<char *>(p.host_stage);
+        std::memcpy(h, b.sys.data(), sizeof(SysDev) * nsys);
+        NBL_CUDA(cudaMemcpyAsync(B.sys, h, sizeof(SysDev) * nsys, cudaMemcpyHostToDevice, st),
+                 "copy systems");
+        h += sizeof(SysDev) * nsys;
+        int64_t *sab = reinterpret_cast<int64_t *>(h);
+        for (int s2 = 0; s2 < nsys; s2++) sab[s2] = b.sys[s2].atom_base;
+        NBL_CUDA(cudaMemcpyAsync(B.sys_atom_base, sab, sizeof(int64_t) * nsys,
+                                 cudaMemcpyHostToDevice, st), "copy systems");
+        h += sizeof(int64_t) * nsys;
+        if (!b.pt64.empty()) {
+            double *p64 = reinterpret_cast<double *>(h);
+            std::memcpy(p64, b.pt64.data(), sizeof(double) * b.pt64.size());
+            h += sizeof(double) * b.pt64.size();
+            float *p32 = reinterpret_cast<float *>(h);
+            for (size_t k = 0; k < b.pt64.size(); k++) p32[k] = (float)b.pt64[k];
+            NBL_CUDA(cudaMemcpyAsync(B.pt64, p64, sizeof(double) * b.pt64.size(),
+                                     cudaMemcpyHostToDevice, st), "copy per-type cutoffs");
+            NBL_CUDA(cudaMemcpyAsync(B.pt32, p32, sizeof(float) * b.pt64.size(),
+                                     cudaMemcpyHostToDevice, st), "copy per-type cutoffs");
+        }
+        NBL_CUDA(cudaEventRecord(p.stage_done, st), "staging event");
+        p.stage_in_flight = true;
+    }
+
+    NBL_CUDA(cudaMemsetAsync(B.small, 0, sizeof(int) * 8, st), "memset");
+    NBL_CUDA(cudaMemsetAsync(B.table, 0, sizeof(int2) * b.table_size, st), "memset table");
+    if (b.grid == kGridHashed)
+        NBL_CUDA(cudaMemsetAsync(B.hkey, 0xff, sizeof(unsigned long long) * b.table_size, st),
+                 "memset hash");
+    NBL_CUDA(cudaMemsetAsync(B.amax, 0, sizeof(float) * nsys, st), "memset");
+
+    int *n_home = B.small + 0;
+    int *err = B.small + 1;
+
+    BinArgs ba;
+    ba.sys = B.sys;
+    ba.sys_atom_base = B.sys_atom_base;
+    ba.nsys = nsys;
+    ba.grid = b.grid;
+    ba.positions = B.pos;
+    ba.natoms = N;
+    ba.keys = B.keys;
+    ba.vals = B.vals;
+    ba.hkey = B.hkey;
+    ba.hmask = (unsigned long long)(b.table_size - 1);
+    ba.err = err;
+    NBL_CUDA(launch_bin(ba, st), "k_bin");
+
+    bool in_alt = false;
+    NBL_CUDA(radix_sort_pairs(B.keys, B.vals, B.keys2, B.vals2, N, b.key_bits, B.hist,
+                              B.hist_scan, B.scan32, st, &in_alt),
+             "radix sort");
+    const uint32_t *skeys = in_alt ? B.keys2 : B.keys;
+    const int32_t *svals = in_alt ? B.vals2 : B.vals;
+
+    GatherArgs ga;
+    ga.sys = B.sys;
+    ga.sys_atom_base = B.sys_atom_base;
+    ga.nsys = nsys;
+    ga.grid = b.grid;
+    ga.positions = B.pos;
+    ga.per_atom = B.per_atom;
+    ga.types = B.types;
+    ga.natoms = N;
+    ga.keys = skeys;
+    ga.vals = svals;
+    ga.table = B.table;
+    ga.pos64 = B.pos64;
+    ga.pos32 = B.pos32;
+    ga.aux = B.aux;
+    ga.amax = B.amax;
+    ga.home = B.home;
+    ga.n_home = n_home;
+    NBL_CUDA(launch_gather(ga, st), "k_gather");
+
+    TraverseArgs &ta = p.targs;
+    std::memset(&ta, 0, sizeof(ta));
+    ta.sys = B.sys;
+    ta.home = B.home;
+    ta.n_home = n_home;
+    ta.grid = b.grid;
+    ta.table = B.table;
+    ta.hkey = B.hkey;
+    ta.hmask = (unsigned long long)(b.table_size - 1);
+    ta.pos64 = B.pos64;
+    ta.pos32 = B.pos32;
+    ta.aux = B.aux;
+    ta.amax = B.amax;
+    ta.pt32 = B.pt32;
+    ta.pt64 = B.pt64;
+    ta.counts = B.counts;
+    ta.offsets = B.offsets;
+    ta.err = err;
+    p.trav_grid = traverse_grid(p, N);
+    NBL_CUDA(launch_traverse(kModeCount, b.fp32, ta, p.trav_grid, st), "count pass");
+    NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
+
+    if (sync) {
+        NBL_CUDA(cudaMemcpyAsync(p.host_small, B.offsets + N, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st), "read pair count");
+        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, B.small, sizeof(int) * 2,
+                                 cudaMemcpyDeviceToHost, st), "read flags");
+        NBL_CUDA(cudaStreamSynchronize(st), "count phase");
+        p.stage_in_flight = false;
+        int flags[2];
+        std::memcpy(flags, p.host_small + 1, sizeof(flags));
+        p.npairs = p.host_small[0];
+        if (flags[1] & kErrRange)
+            return set_error(NBL_ERROR_RANGE,
+                             "positions must be finite and within 2^29 cells of the box");
+        if (flags[1] & kErrInternal)
+            return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded in count phase");
+    }
+    p.have_count = true;
+    return NBL_SUCCESS;
+}
+
+nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_t st) {
+    if (!p.have_count)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "nbl_fill without a preceding nbl_count");
+    TraverseArgs ta = p.targs;
+    ta.first = o.first;
+    ta.second = o.second;
+    ta.distvec = o.distvec;
+    ta.absdist = o.absdist;
+    ta.shift = o.shift;
+    ta.capacity = capacity;
+    if (!(o.first || o.second || o.distvec || o.absdist || o.shift)) return NBL_SUCCESS;
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, ta, p.trav_grid, st), "fill pass");
+    return NBL_SUCCESS;
+}
+
+nbl_status read_flags(Plan &p, cudaStream_t st) {
+    NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, p.bufs.small, sizeof(int) * 2,
+                             cudaMemcpyDeviceToHost, st), "read flags");
+    NBL_CUDA(cudaStreamSynchronize(st), "check");
+    int flags[2];
+    std::memcpy(flags, p.host_small + 1, sizeof(flags));
+    if (flags[1] & kErrRange)
+        return set_error(NBL_ERROR_RANGE,
+                         "positions must be finite and within 2^29 cells of the box");
+    if (flags[1] & kErrCapacity)
+        return set_error(NBL_ERROR_CAPACITY, "output capacity smaller than the pair count");
+    if (flags[1] & kErrInternal)
+        return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded");
+    return NBL_SUCCESS;
+}
+
+// Request -> one-system batch.
+nbl_status batch_from_request(const nbl_request *req, Batch &b) {
+    if (!req) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null request");
+    if (req->quantities & ~31)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "Unsupported quantity specified.");
+    if (req->nat < 0) return set_error(NBL_ERROR_INVALID_ARGUMENT, "negative atom count");
+    if (!req->cell_origin || !req->cell || !req->inv_cell || !req->pbc)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "missing geometry");
+    if (req->nat > 0 && !req->positions)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "missing positions");
+    if (req->per_type_cutoff_sq && req->ncutoffs < 0)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "negative ncutoffs");
+    if (req->precision != NBL_PRECISION_FP32_FILTER && req->precision != NBL_PRECISION_FP64)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "unknown precision");
+    if (req->grid < NBL_GRID_AUTO || req->grid > NBL_GRID_HASHED)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "unknown grid");
+    b = Batch();
+    SysDev S;
+    int64_t ncells = 0;
+    nbl_status st = plan_system(req->cell_origin, req->cell, req->inv_cell, req->pbc,
+                                req->cutoff, S, ncells);
+    if (st != NBL_SUCCESS) return st;
+    S.nat = (int32_t)req->nat;
+    S.atom_base = 0;
+    if (req->per_atom_cutoff) {
+        S.cutoff_kind = kCutPerAtom;
+    } else if (req->per_type_cutoff_sq && req->types) {
+        S.cutoff_kind = kCutPerType;
+        S.ncutoffs = req->ncutoffs;
+        S.pt_base = 0;
+        b.pt64.assign(req->per_type_cutoff_sq,
+                      req->per_type_cutoff_sq + (size_t)req->ncutoffs * req->ncutoffs);
+    } else {
+        S.cutoff_kind = kCutScalar;
+    }
+    b.sys.push_back(S);
+    b.ncells.push_back(ncells);
+    b.natoms = req->nat;
+    b.positions = req->positions;
+    b.pos_on_device = req->positions_on_device != 0;
+    b.per_atom = S.cutoff_kind == kCutPerAtom ? req->per_atom_cutoff : nullptr;
+    b.types = S.cutoff_kind == kCutPerType ? req->types : nullptr;
+    b.aux_on_device = req->aux_on_device != 0;
+    b.fp32 = req->precision == NBL_PRECISION_FP32_FILTER;
+    b.quantities = req->quantities;
+    return finish_batch(b, req->grid);
+}
+
+// RAII device switch.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        int cur = 0;
+        if (cudaGetDevice(&cur) != cudaSuccess) {
+            ok = false;
+            return;
+        }
+        if (dev >= 0 && dev != cur) {
+            if (cudaSetDevice(dev) != cudaSuccess) ok = false;
+            prev = cur;
+        }
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+nbl_status plan_init(Plan &p, int device_id) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_error(NBL_ERROR_NO_DEVICE, "no CUDA device available");
+    }
+    int dev = device_id;
+    if (dev < 0) NBL_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev >= ndev) return set_error(NBL_ERROR_INVALID_ARGUMENT, "no device %d", dev);
+    p.device = dev;
+    DeviceGuard g(dev);
+    NBL_CUDA(cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, dev),
+             "device query");
+    NBL_CUDA(cudaMallocHost(&p.host_small, sizeof(int64_t) * 4), "pinned");
+    NBL_CUDA(cudaEventCreateWithFlags(&p.stage_done, cudaEventDisableTiming), "event");
+    return NBL_SUCCESS;
+}
+
+void plan_free(Plan &p) {
+    DeviceGuard g(p.device);
+    if (p.stage_done) cudaEventSynchronize(p.stage_done);
+    p.ws.release();
+    if (p.host_small) cudaFreeHost(p.host_small);
+    if (p.host_stage) cudaFreeHost(p.host_stage);
+    if (p.stage_done) cudaEventDestroy(p.stage_done);
+    p.host_small = nullptr;
+    p.host_stage = nullptr;
+    p.stage_done = nullptr;
+}
+
+}  // namespace nbl
+
+using namespace nbl;
+
+struct nbl_plan {
+    Plan p;
+};
+
+extern "C" {
+
+nbl_status nbl_plan_create(int device_id, nbl_plan **plan) {
+    clear_error();
+    if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan pointer");
+    *plan = nullptr;
+    nbl_plan *np = new (std::nothrow) nbl_plan();
+    if (!np) return set_error(NBL_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    nbl_status st = plan_init(np->p, device_id);
+    if (st != NBL_SUCCESS) {
+        plan_free(np->p);
+        delete np;
+        return st;
+    }
+    *plan = np;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_plan_destroy(nbl_plan *plan) {
+    clear_error();
+    if (!plan) return NBL_SUCCESS;
+    plan_free(plan->p);
+    delete plan;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_plan_trim(nbl_plan *plan) {
+    clear_error();
+    if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan");
+    DeviceGuard g(plan->p.device);
+    cudaDeviceSynchronize();
+    plan->p.ws.release();
+    plan->p.have_count = false;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_count(nbl_plan *plan, const nbl_request *req, void *stream,
+                     int64_t *npairs) {
+    clear_error();
+    if (!plan || !npairs) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    *npairs = 0;
+    plan->p.have_count = false;
+    Batch b;
+    nbl_status st = batch_from_request(req, b);
+    if (st != NBL_SUCCESS) return st;
+    if (req->device_id >= 0 && req->device_id != plan->p.device)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "request device %d != plan device %d",
+                         req->device_id, plan->p.device);
+    DeviceGuard g(plan->p.device);
+    if (!g.ok) return set_error(NBL_ERROR_CUDA, "cannot select device %d", plan->p.device);
+    st = run_count(plan->p, b, static_cast<cudaStream_t>(stream), true);
+    if (st != NBL_SUCCESS) return st;
+    plan->p.quantities = req->quantities;
+    *npairs = plan->p.npairs;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_fill(nbl_plan *plan, const nbl_outputs *out, void *stream) {
+    clear_error();
+    if (!plan || !out) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(plan->p.device);
+    return run_fill(plan->p, *out, plan->p.npairs, static_cast<cudaStream_t>(stream));
+}
+
+nbl_status nbl_fill_host(nbl_plan *plan, const nbl_outputs *host_out, void *stream) {
+    clear_error();
+    if (!plan || !host_out) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    Plan &p = plan->p;
+    if (!p.have_count)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "nbl_fill_host without nbl_count");
+    DeviceGuard g(p.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t np = p.npairs;
+    if (np == 0) return NBL_SUCCESS;
+    const nbl_outputs &h = *host_out;
+    Layout L;
+    size_t o_i = h.first ? L.add(sizeof(int32_t) * np) : 0;
+    size_t o_j = h.second ? L.add(sizeof(int32_t) * np) : 0;
+    size_t o_D = h.distvec ? L.add(sizeof(double) * 3 * np) : 0;
+    size_t o_d = h.absdist ? L.add(sizeof(double) * np) : 0;
+    size_t o_S = h.shift ? L.add(sizeof(int32_t) * 3 * np) : 0;
+    nbl_status s = ensure(p.ws.out_base, p.ws.out_bytes, std::max<size_t>(L.total, 256),
+                          "output scratch");
+    if (s != NBL_SUCCESS) return s;
+    char *base = static_cast<char *>(p.ws.out_base);
+    nbl_outputs d;
+    d.first = h.first ? (int32_t *)(base + o_i) : nullptr;
+    d.second = h.second ? (int32_t *)(base + o_j) : nullptr;
+    d.distvec = h.distvec ? (double *)(base + o_D) : nullptr;
+    d.absdist = h.absdist ? (double *)(base + o_d) : nullptr;
+    d.shift = h.shift ? (int32_t *)(base + o_S) : nullptr;
+    s = run_fill(p, d, np, st);
+    if (s != NBL_SUCCESS) return s;
+    if (h.first)
+        NBL_CUDA(cudaMemcpyAsync(h.first, d.first, sizeof(int32_t) * np,
+                                 cudaMemcpyDeviceToHost, st), "copy i");
+    if (h.second)
+        NBL_CUDA(cudaMemcpyAsync(h.second, d.second, sizeof(int32_t) * np,
+                                 cudaMemcpyDeviceToHost, st), "copy j");
+    if (h.distvec)
+        NBL_CUDA(cudaMemcpyAsync(h.distvec, d.distvec, sizeof(double) * 3 * np,
+                                 cudaMemcpyDeviceToHost, st), "copy D");
+    if (h.absdist)
+        NBL_CUDA(cudaMemcpyAsync(h.absdist, d.absdist, sizeof(double) * np,
+                                 cudaMemcpyDeviceToHost, st), "copy d");
+    if (h.shift)
+        NBL_CUDA(cudaMemcpyAsync(h.shift, d.shift, sizeof(int32_t) * 3 * np,
+                                 cudaMemcpyDeviceToHost, st), "copy S");
+    return read_flags(p, st);
+}
+
+nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
+                           double *dist, int32_t *count, int *overflow, void *stream) {
+    clear_error();
+    if (!plan || !idx || !dist || !count || !overflow || max_neighbours <= 0)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "bad neighbour-matrix arguments");
+    Plan &p = plan->p;
+    if (!p.have_count) return set_error(NBL_ERROR_INVALID_ARGUMENT, "no count phase");
+    DeviceGuard g(p.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = p.batch_natoms;
+    const size_t nk = (size_t)n * (size_t)max_neighbours;
+    *overflow = 0;
+    if (n == 0) return NBL_SUCCESS;
+    NBL_CUDA(cudaMemsetAsync(idx, 0, sizeof(int32_t) * nk, st), "memset matrix");
+    NBL_CUDA(cudaMemsetAsync(dist, 0, sizeof(double) * 3 * nk, st), "memset matrix");
+    NBL_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t) * n, st), "memset matrix");
+    NBL_CUDA(cudaMemsetAsync(p.bufs.small + 2, 0, sizeof(int), st), "memset flag");
+    TraverseArgs ta = p.targs;
+    ta.mat_k = max_neighbours;
+    ta.mat_idx = idx;
+    ta.mat_dist = dist;
+    ta.mat_count = count;
+    ta.mat_overflow = p.bufs.small + 2;
+    ta.capacity = 0;
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, ta, p.trav_grid, st), "matrix fill");
+    NBL_CUDA(cudaMemcpyAsync(p.host_small + 2, p.bufs.small + 2, sizeof(int),
+                             cudaMemcpyDeviceToHost, st), "read overflow");
+    nbl_status r = read_flags(p, st);
+    int ov = 0;
+    std::memcpy(&ov, p.host_small + 2, sizeof(int));
+    *overflow = ov ? 1 : 0;
+    return r;
+}
+
+nbl_status nbl_counts(nbl_plan *plan, int32_t *counts, void *stream) {
+    clear_error();
+    if (!plan || !counts) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    Plan &p = plan->p;
+    if (!p.have_count) return set_error(NBL_ERROR_INVALID_ARGUMENT, "no count phase");
+    DeviceGuard g(p.device);
+    if (p.batch_natoms > 0)
+        NBL_CUDA(cudaMemcpyAsync(counts, p.bufs.counts, sizeof(int32_t) * p.batch_natoms,
+                                 cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)),
+                 "copy counts");
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_row_offsets(nbl_plan *plan, int64_t *offsets, void *stream) {
+    clear_error();
+    if (!plan || !offsets) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    Plan &p = plan->p;
+    if (!p.have_count) return set_error(NBL_ERROR_INVALID_ARGUMENT, "no count phase");
+    DeviceGuard g(p.device);
+    NBL_CUDA(cudaMemcpyAsync(offsets, p.bufs.offsets, sizeof(int64_t) * (p.batch_natoms + 1),
+                             cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)),
+             "copy offsets");
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_check(nbl_plan *plan, void *stream) {
+    clear_error();
+    if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan");
+    DeviceGuard g(plan->p.device);
+    return read_flags(plan->p, static_cast<cudaStream_t>(stream));
+}
+
+nbl_status nbl_neighbour_list_device(const nbl_request *req, void *stream,
+                                     nbl_device_result *result) {
+    clear_error();
+    if (!req || !result) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    std::memset(result, 0, sizeof(*result));
+    // One cached plan per (host thread, device).
+    static thread_local std::vector<nbl_plan *> plans;
+    int dev = req->device_id;
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(NBL_ERROR_NO_DEVICE, "no CUDA device available");
+        }
+    }
+    if ((int)plans.size() <= dev) plans.resize(dev + 1, nullptr);
+    if (!plans[dev]) {
+        nbl_status st = nbl_plan_create(dev, &plans[dev]);
+        if (st != NBL_SUCCESS) return st;
+    }
+    nbl_plan *plan = plans[dev];
+    int64_t np = 0;
+    nbl_status st = nbl_count(plan, req, stream, &np);
+    if (st != NBL_SUCCESS) return st;
+    DeviceGuard g(dev);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    result->npairs = np;
+    result->device_id = dev;
+    const int q = req->quantities;
+    const size_t n1 = std::max<int64_t>(np, 1);
+    nbl_outputs o;
+    std::memset(&o, 0, sizeof(o));
+    if (q & NBL_QUANTITY_FIRST)
+        NBL_CUDA(cudaMallocAsync((void **)&result->first, sizeof(int32_t) * n1, s), "alloc i");
+    if (q & NBL_QUANTITY_SECOND)
+        NBL_CUDA(cudaMallocAsync((void **)&result->second, sizeof(int32_t) * n1, s), "alloc j");
+    if (q & NBL_QUANTITY_DISTVEC)
+        NBL_CUDA(cudaMallocAsync((void **)&result->distvec, sizeof(double) * 3 * n1, s),
+                 "alloc D");
+    if (q & NBL_QUANTITY_ABSDIST)
+        NBL_CUDA(cudaMallocAsync((void **)&result->absdist, sizeof(double) * n1, s), "alloc d");
+    if (q & NBL_QUANTITY_SHIFT)
+        NBL_CUDA(cudaMallocAsync((void **)&result->shift, sizeof(int32_t) * 3 * n1, s),
+                 "alloc S");
+    o.first = result->first;
+    o.second = result->second;
+    o.distvec = result->distvec;
+    o.absdist = result->absdist;
+    o.shift = result->shift;
+    return run_fill(plan->p, o, np, s);
+}
+
+nbl_status nbl_device_result_free(nbl_device_result *r, void *stream) {
+    clear_error();
+    if (!r) return NBL_SUCCESS;
+    DeviceGuard g(r->device_id);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (r->first) cudaFreeAsync(r->first, s);
+    if (r->second) cudaFreeAsync(r->second, s);
+    if (r->distvec) cudaFreeAsync(r->distvec, s);
+    if (r->absdist) cudaFreeAsync(r->absdist, s);
+    if (r->shift) cudaFreeAsync(r->shift, s);
+    std::memset(r, 0, sizeof(*r));
+    return NBL_SUCCESS;
+}
+
+const char *nbl_last_error(void) { return g_last_error.c_str(); }
+
+long long nbl_launch_count(int reset) {
+    const long long n = g_launches;
+    if (reset) g_launches = 0;
+    return n;
+}
+
+int nbl_has_gpu(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0 ? 1 : 0;
+}
+
+int nbl_device_type(void) { return 2; }
+
+const char *nbl_version(void) { return "nbl_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// nbl_build.cuh -- argument blocks and launchers of the pair kernels.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "nbl_internal.cuh"
+
+namespace nbl {
+
+constexpr int kModeCount = 0;
+constexpr int kModeFill = 1;
+
+struct BinArgs {
+    const SysDev *sys;
+    const int64_t *sys_atom_base;
+    int nsys;
+    int grid;
+    const double *positions;  // [3*natoms], concatenated systems
+    int64_t natoms;
+    uint32_t *keys;
+    int32_t *vals;
+    unsigned long long *hkey;
+    unsigned long long hmask;
+    int *err;
+};
+
+struct GatherArgs {
+    const SysDev *sys;
+    const int64_t *sys_atom_base;
+    int nsys;
+    int grid;
+    const double *positions;
+    const double *per_atom;   // [natoms] or null
+    const int32_t *types;     // [natoms] or null
+    int64_t natoms;
+    const uint32_t *keys;     // sorted
+    const int32_t *vals;      // sorted: global atom index
+    int2 *table;
+    double4 *pos64;
+    float4 *pos32;
+    int4 *aux;
+    float *amax;              // [nsys], zeroed
+    HomeCell *home;
+    int *n_home;              // zeroed
+};
+
+struct TraverseArgs {
+    const SysDev *sys;
+    const HomeCell *home;
+    const int *n_home;
+    int grid;
+    const int2 *table;
+    const unsigned long long *hkey;
+    unsigned long long hmask;
+    const double4 *pos64;
+    const float4 *pos32;
+    const int4 *aux;
+    const float *amax;
+    const float *pt32;        // per-type squared cutoffs, FP32
+    const double *pt64;       // per-type squared cutoffs, FP64
+    int32_t *counts;          // COUNT: per global atom
+    const int64_t *offsets;   // FILL: row starts per global atom (+1)
+    int32_t *first;
+    int32_t *second;
+    double *distvec;
+    double *absdist;
+    int32_t *shift;
+    int64_t capacity;
+    // Dense-matrix sink (neighbour_matrix): when mat_k > 0 the fill pass writes
+    // row (global atom index) a, slot s < mat_k of mat_idx / mat_dist instead
+    // of the pair list, and mat_count[a] = row length.
+    int32_t mat_k;
+    int32_t *mat_idx;
+    double *mat_dist;
+    int32_t *mat_count;
+    int *mat_overflow;
+    int *err;
+};
+
+cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
+cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
+cudaError_t launch_traverse(int mode, bool fp32, const TraverseArgs &a, int grid,
+                            cudaStream_t st);
+
+}  // namespace nbl

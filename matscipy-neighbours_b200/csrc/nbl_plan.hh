@@ -1,0 +1,97 @@
+// nbl_plan.hh -- host-side state of the engine (plans, batches, workspace).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "nbl_b200.h"
+#include "nbl_build.cuh"
+#include "nbl_internal.cuh"
+
+namespace nbl {
+
+// A batch of independent systems planned on the host.
+struct Batch {
+    std::vector<SysDev> sys;
+    std::vector<int64_t> ncells;
+    std::vector<double> pt64;      // concatenated per-type squared cutoffs
+    int64_t natoms = 0;
+    const double *positions = nullptr;
+    bool pos_on_device = false;
+    const double *per_atom = nullptr;
+    const int32_t *types = nullptr;
+    bool aux_on_device = false;
+    int grid = kGridDense;         // resolved kGrid*
+    int64_t table_size = 1;
+    int key_bits = 0;
+    bool fp32 = true;
+    int quantities = 0;
+};
+
+// Device buffers of one call, carved out of the workspace.
+struct Bufs {
+    double *pos = nullptr;
+    double *per_atom = nullptr;
+    int32_t *types = nullptr;
+    SysDev *sys = nullptr;
+    int64_t *sys_atom_base = nullptr;
+    double *pt64 = nullptr;
+    float *pt32 = nullptr;
+    uint32_t *keys = nullptr, *keys2 = nullptr;
+    int32_t *vals = nullptr, *vals2 = nullptr;
+    int32_t *hist = nullptr, *hist_scan = nullptr, *scan32 = nullptr;
+    int64_t *scan64 = nullptr;
+    int2 *table = nullptr;
+    unsigned long long *hkey = nullptr;
+    double4 *pos64 = nullptr;
+    float4 *pos32 = nullptr;
+    int4 *aux = nullptr;
+    float *amax = nullptr;
+    HomeCell *home = nullptr;
+    int32_t *counts = nullptr;
+    int64_t *offsets = nullptr;
+    int *small = nullptr;  // [0] occupied cells, [1] error bits
+};
+
+struct Workspace {
+    void *base = nullptr;
+    size_t bytes = 0;
+    void *out_base = nullptr;  // device output scratch of nbl_fill_host
+    size_t out_bytes = 0;
+    void release();
+};
+
+struct Plan {
+    int device = 0;
+    int num_sms = 148;
+    Workspace ws;
+    Bufs bufs;
+    TraverseArgs targs{};
+    int trav_grid = 0;
+    int64_t batch_natoms = 0;
+    int batch_nsys = 0;
+    bool batch_fp32 = true;
+    int batch_grid = kGridDense;
+    bool have_count = false;
+    int64_t npairs = 0;
+    int quantities = 0;
+    int64_t *host_small = nullptr;  // pinned: [0] pair count, [1] flags
+    void *host_stage = nullptr;     // pinned staging of the small host tables
+    size_t host_stage_bytes = 0;
+    cudaEvent_t stage_done = nullptr;
+    bool stage_in_flight = false;
+};
+
+nbl_status set_error(nbl_status st, const char *fmt, ...);
+nbl_status cuda_status(cudaError_t e, const char *where);
+nbl_status plan_system(const double origin[3], const double cell[9],
+                       const double inv_cell[9], const uint8_t pbc[3], double cutoff,
+                       SysDev &S, int64_t &ncells);
+nbl_status finish_batch(Batch &b, int grid_req);
+nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync);
+nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_t st);
+nbl_status read_flags(Plan &p, cudaStream_t st);
+
+}  // namespace nbl

@@ -1,0 +1,281 @@
+// nbl_sort.cu -- hand-written device exclusive scan and stable LSD radix sort.
+//
+// Replace the reference's CUB calls (src/libneighbours/device_primitives.cc:
+// 31-86: DeviceScan::ExclusiveSum with a temp cudaMalloc and two blocking D2H
+// reads per call; DeviceRadixSort::SortPairs).  Here nothing allocates or
+// synchronises: all scratch comes from the caller's workspace, so the whole
+// pipeline can be captured in a CUDA graph.
+//
+// Scan: three-phase (tile reduce -> recursive scan of tile sums -> tile scan
+// with carry-in); no inter-block waiting, so no spin loops at all.
+// Sort: 8-bit digits; per pass one histogram kernel, one scan of the
+// digit-major histogram and one stable scatter kernel.  Stability (needed so
+// that the atoms of one cell stay in ascending index order, exactly as the
+// reference's counting sort leaves them) comes from ranking keys in index
+// order inside each tile with __match_any_sync.
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "nbl_internal.cuh"
+#include "nbl_sort.cuh"
+
+namespace nbl {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        T o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += o;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T &total, T *s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    T incl = warp_incl_scan(v);
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nwarps ? s_warp[lane] : T(0);
+        T wi = warp_incl_scan(w);
+        if (lane < nwarps) s_warp[lane] = wi - w;
+        if (lane == nwarps - 1) s_warp[32] = wi;
+    }
+    __syncthreads();
+    T r = incl - v + s_warp[warp];
+    total = s_warp[32];
+    __syncthreads();
+    return r;
+}
+
+template <typename Tin, typename Tacc>
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_reduce(const Tin *__restrict__ in, int64_t n, Tacc *__restrict__ sums) {
+    __shared__ Tacc s_warp[33];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    Tacc acc = 0;
+#pragma unroll
+    for (int it = 0; it < kScanItems; it++) {
+        int64_t idx = base + (int64_t)it * kScanThreads + threadIdx.x;
+        if (idx < n) acc += (Tacc)in[idx];
+    }
+    Tacc total;
+    block_excl_scan<Tacc>(acc, total, s_warp);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// Exclusive scan of one tile (blocked: thread t owns items t*8 .. t*8+7) with
+// an optional carry-in per tile; writes out[n] = grand total when
+// `write_total`.
+template <typename Tin, typename Tacc>
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_tile(const Tin *__restrict__ in, int64_t n, Tacc *__restrict__ out,
+            const Tacc *__restrict__ carry, int write_total) {
+    __shared__ Tacc s_warp[33];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile +
+                         (int64_t)threadIdx.x * kScanItems;
+    Tacc v[kScanItems];
+    Tacc local = 0;
+#pragma unroll
+    for (int it = 0; it < kScanItems; it++) {
+        int64_t idx = base + it;
+        v[it] = idx < n ? (Tacc)in[idx] : Tacc(0);
+        local += v[it];
+    }
+    Tacc total;
+    Tacc run = block_excl_scan<Tacc>(local, total, s_warp);
+    const Tacc c = carry ? carry[blockIdx.x] : Tacc(0);
+    run += c;
+#pragma unroll
+    for (int it = 0; it < kScanItems; it++) {
+        int64_t idx = base + it;
+        if (idx < n) out[idx] = run;
+        run += v[it];
+    }
+    if (write_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+        out[n] = c + total;
+}
+
+}  // namespace
+
+int64_t scan_scratch_elems(int64_t n) {
+    int64_t total = 0;
+    while (n > kScanTile) {
+        int64_t tiles = (n + kScanTile - 1) / kScanTile;
+        total += 2 * tiles + 1;
+        n = tiles;
+    }
+    return total + 1;
+}
+
+template <typename Tin, typename Tacc>
+static cudaError_t scan_rec(const Tin *in, int64_t n, Tacc *out, int write_total,
+                            Tacc *scratch, cudaStream_t st) {
+    if (n <= 0) {
+        if (write_total) return cudaMemsetAsync(out, 0, sizeof(Tacc), st);
+        return cudaSuccess;
+    }
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        k_scan_tile<Tin, Tacc><<<1, kScanThreads, 0, st>>>(in, n, out, nullptr,
+                                                          write_total);
+        count_launch();
+        return cudaGetLastError();
+    }
+    Tacc *sums = scratch;
+    Tacc *carry = scratch + tiles;
+    k_scan_reduce<Tin, Tacc><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, sums);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_rec<Tacc, Tacc>(sums, tiles, carry, 0, scratch + 2 * tiles + 1, st);
+    if (e != cudaSuccess) return e;
+    k_scan_tile<Tin, Tacc><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, out, carry,
+                                                                   write_total);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t exclusive_scan_i32_i64(const int32_t *in, int64_t n, int64_t *out,
+                                   int64_t *scratch, cudaStream_t st) {
+    return scan_rec<int32_t, int64_t>(in, n, out, 1, scratch, st);
+}
+
+cudaError_t exclusive_scan_i32_i32(const int32_t *in, int64_t n, int32_t *out,
+                                   int32_t *scratch, cudaStream_t st) {
+    return scan_rec<int32_t, int32_t>(in, n, out, 0, scratch, st);
+}
+
+// ---- radix sort -----------------------------------------------------------
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortIters = 16;                               // per warp
+constexpr int kSortTile = kSortThreads * kSortIters;         // 4096
+constexpr int kRadix = 256;
+
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_hist(const uint32_t *__restrict__ keys, int64_t n, int shift,
+             int32_t *__restrict__ hist, int ntiles) {
+    __shared__ int32_t s_cnt[kRadix];
+    s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int it = 0; it < kSortIters; it++) {
+        int64_t idx = base + (int64_t)it * kSortThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&s_cnt[(keys[idx] >> shift) & 0xffu], 1);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = s_cnt[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_scatter(const uint32_t *__restrict__ kin, const int32_t *__restrict__ vin,
+                uint32_t *__restrict__ kout, int32_t *__restrict__ vout, int64_t n,
+                int shift, const int32_t *__restrict__ hoff, int ntiles) {
+    __shared__ int32_t s_wc[kSortWarps][kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads)
+        (&s_wc[0][0])[i] = 0;
+    __syncthreads();
+
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortIters);
+    uint32_t key[kSortIters];
+    int32_t val[kSortIters];
+    int32_t rank[kSortIters];
+#pragma unroll
+    for (int it = 0; it < kSortIters; it++) {
+        const int64_t idx = wbase + it * 32 + lane;
+        const bool valid = idx < n;
+        key[it] = valid ? kin[idx] : 0u;
+        val[it] = valid ? vin[idx] : 0;
+        // Invalid lanes get a private pseudo-digit so they never match.
+        const uint32_t d = valid ? ((key[it] >> shift) & 0xffu) : (kRadix + lane);
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        int r = 0;
+        if (valid) r = s_wc[warp][d] + __popc(peers & lt);
+        __syncwarp();
+        if (valid && (peers & lt) == 0) s_wc[warp][d] += __popc(peers);
+        __syncwarp();
+        rank[it] = r;
+    }
+    __syncthreads();
+    // Exclusive prefix over warps, per digit.
+    {
+        const int d = threadIdx.x;
+        int32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; w++) {
+            int32_t c = s_wc[w][d];
+            s_wc[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kSortIters; it++) {
+        const int64_t idx = wbase + it * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[it] >> shift) & 0xffu;
+            const int64_t pos = (int64_t)hoff[(int64_t)d * ntiles + blockIdx.x] +
+                                s_wc[warp][d] + rank[it];
+            kout[pos] = key[it];
+            vout[pos] = val[it];
+        }
+    }
+}
+
+}  // namespace
+
+int64_t radix_hist_elems(int64_t n) {
+    const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+    return tiles * kRadix;
+}
+
+cudaError_t radix_sort_pairs(uint32_t *keys, int32_t *vals, uint32_t *keys_alt,
+                             int32_t *vals_alt, int64_t n, int bits,
+                             int32_t *hist, int32_t *hist_scan,
+                             int32_t *scan_scratch, cudaStream_t st,
+                             bool *result_in_alt) {
+    *result_in_alt = false;
+    if (n <= 1 || bits <= 0) return cudaSuccess;
+    const int ntiles = (int)((n + kSortTile - 1) / kSortTile);
+    uint32_t *ka = keys, *kb = keys_alt;
+    int32_t *va = vals, *vb = vals_alt;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(ka, n, shift, hist, ntiles);
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        e = exclusive_scan_i32_i32(hist, (int64_t)ntiles * kRadix, hist_scan,
+                                   scan_scratch, st);
+        if (e != cudaSuccess) return e;
+        k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(ka, va, kb, vb, n, shift,
+                                                         hist_scan, ntiles);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        uint32_t *tk = ka; ka = kb; kb = tk;
+        int32_t *tv = va; va = vb; vb = tv;
+        *result_in_alt = !*result_in_alt;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace nbl
