@@ -187,6 +187,24 @@ NBL_API nbl_status nbl_neighbour_list_device(const nbl_request *req, void *strea
                                      nbl_device_result *result);
 NBL_API nbl_status nbl_device_result_free(nbl_device_result *result, void *stream);
 
+/* Allocation-free variant of nbl_count + nbl_fill, for callers that cannot
+   allocate device memory at call time (an MD loop that forbids allocation
+   after start-up, a host whose pool allocator has reserved the device
+   memory).  No counterpart in the reference.  All scratch lives in one static
+   8 MiB __device__ array inside the library, held by every GPU that loads it
+   until exit; at most NBL_NOALLOC_MAX_ATOMS atoms.  Inputs as in nbl_request
+   (positions device or host); `out` holds caller-allocated DEVICE buffers of
+   `capacity` pairs.  Sets *npairs and returns NBL_ERROR_CAPACITY (writing
+   nothing) when npairs > capacity.  Synchronises `stream`.  Calls overlapping
+   on the GPU race on the shared scratch: serialise them.  The first call on a
+   device resolves the scratch address (device must be current) and should
+   come before any stream capture. */
+#define NBL_NOALLOC_MAX_ATOMS 32768
+NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
+                                              const nbl_outputs *out,
+                                              int64_t capacity, int64_t *npairs,
+                                              void *stream);
+
 /* Last error message of the calling thread ("" if none). */
 NBL_API const char *nbl_last_error(void);
 
