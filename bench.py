@@ -75,58 +75,61 @@ def _traffic_per_launch(npairs, nat):
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    """SM clock and throttle reasons sampled every 20 ms during the timed region
+    (read-only NVML queries; nvidia-smi as a fallback)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event-reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, torch_device):
+        self.dev = torch_device
+        self.samples = []
+        self.reasons = set()
+        self.sm_max = None
+        self._stop = threading.Event()
+        self._thread = None
+        self.handle = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(torch_device)
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.sm_max = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle,
+                                                                 pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.handle = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(self.nvml.nvmlDeviceGetClockInfo(
+                    self.handle, self.nvml.NVML_CLOCK_SM)))
+                bits = int(self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                for b, name in self.REASONS.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.02)
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except Exception:
-            self.proc = None
-
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+        if self.handle is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.thread.join(timeout=2)
-        sm, smax, reasons = [], None, set()
-        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names[1:], f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self._thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"],
+                    "samples": 0}
+        self._stop.set()
+        self._thread.join(timeout=2)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.sm_max, "reasons": sorted(self.reasons),
+                "samples": len(self.samples), "source": "nvml, 20 ms"}
 
 
 def cpu_baseline(steps=2):
@@ -157,12 +160,16 @@ def cpu_baseline(steps=2):
 
 
 def run_reference(args, rank):
+    """The reference's own CPU core, every host thread.  Each step is a bounded
+    sample of the workload: the same lattice, shear, jitter and cutoff at 32^3
+    unit cells (131,072 atoms, 1/8 of the benchmark size), so that K steps stay
+    within a few minutes; pairs/s is the rate the core sustains."""
     if rank != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     from matscipy_neighbours import _workloads as W
-    w = W.fcc_bulk(seed=0)
+    w = W.fcc_bulk(seed=0, reps=32)
     cores = len(os.sched_getaffinity(0))
     if O.ref_available():
         kind = "reference"
@@ -171,7 +178,7 @@ def run_reference(args, rank):
     else:
         kind, cores = "port", 1
         fn = O.oracle_neighbour_list
-    for _ in range(args.warmup):
+    for _ in range(max(1, min(args.warmup, 3))):
         fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])
     times, npairs = [], 0
     for _ in range(args.steps):
@@ -187,7 +194,8 @@ def run_reference(args, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(WORKLOAD, parallelism="host threads"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"full workload ({npairs} pairs) per step"},
+                         "sample": f"1/8 of the workload per step: 32^3 FCC cells, "
+                                   f"131072 atoms, {npairs} pairs"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -195,10 +203,15 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--reps", type=int, default=64,
+                    help="FCC unit cells per edge (64 = the benchmark size; smaller "
+                         "values make the small cases used for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -227,7 +240,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    w = W.fcc_bulk(seed=rank)
+    w = W.fcc_bulk(seed=rank, reps=args.reps)
     nat = w["positions"].shape[0]
     cell = np.ascontiguousarray(w["cell"])
     inv = np.ascontiguousarray(np.linalg.inv(cell.T))
@@ -282,7 +295,7 @@ def main():
     # --- FP32-filter path (the headline), then plain FP64 for comparison ----
     timed_steps(req, args.warmup)
     ext.check(ext.lib.nbl_check(plan, sptr))
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -296,9 +309,11 @@ def main():
     clk = clocks.stop()
     ext.check(ext.lib.nbl_check(plan, sptr))
 
-    req64 = request("fp64")
-    timed_steps(req64, 2)
-    step64, fill64 = timed_steps(req64, max(3, args.steps // 2))
+    step64 = fill64 = None
+    if not args.no_fp64:
+        req64 = request("fp64")
+        timed_steps(req64, 2)
+        step64, fill64 = timed_steps(req64, max(3, min(args.steps, 20)))
 
     total_ms = sum(step_ms)
     pairs_job = npairs * args.steps
@@ -311,27 +326,31 @@ def main():
     value = pairs_job / (total_ms * 1e-3)
 
     # --- end to end through the public API with host buffers ----------------
-    host_pos = ext.host_empty((nat, 3), np.float64)
-    host_pos[...] = w["positions"]
+    e2e_value = None
     e2e_times = []
-    for k in range(args.warmup + args.steps):
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        res = m.neighbour_list("ijdDS", positions=host_pos, cell=cell, pbc=w["pbc"],
-                               cutoff=w["cutoff"])
-        t1 = time.perf_counter()
-        if k >= args.warmup:
-            e2e_times.append(t1 - t0)
-        del res
-    e2e_total = sum(e2e_times)
-    e2e_pairs = npairs * len(e2e_times)
-    if dist is not None:
-        t = torch.tensor([e2e_total, float(e2e_pairs)], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        e2e_total, e2e_pairs = float(tmax[0]), float(t[1])
-    e2e_value = e2e_pairs / e2e_total
+    if not args.no_e2e:
+        host_pos = ext.host_empty((nat, 3), np.float64)
+        host_pos[...] = w["positions"]
+        e2e_steps = min(args.steps, 10)
+        for k in range(args.warmup + e2e_steps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            res = m.neighbour_list("ijdDS", positions=host_pos, cell=cell, pbc=w["pbc"],
+                                   cutoff=w["cutoff"])
+            t1 = time.perf_counter()
+            if k >= args.warmup:
+                e2e_times.append(t1 - t0)
+            del res
+        e2e_total = sum(e2e_times)
+        e2e_pairs = npairs * len(e2e_times)
+        if dist is not None:
+            t = torch.tensor([e2e_total, float(e2e_pairs)], dtype=torch.float64,
+                             device=dev)
+            tmax = t.clone()
+            dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+            e2e_total, e2e_pairs = float(tmax[0]), float(t[1])
+        e2e_value = e2e_pairs / e2e_total
 
     if rank != 0:
         if dist is not None:
@@ -347,7 +366,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, npairs_per_step=npairs, parallelism=f"replicas{world}",
+        "config": dict(WORKLOAD, natoms=nat, reps=args.reps, npairs_per_step=npairs,
+                       parallelism=f"replicas{world}",
                        l2="flushed between steps (256 MiB write, outside the events)",
                        precision="fp32 filter + fp64 guard-band recheck"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -356,19 +376,20 @@ def main():
                      "kernel": "k_traverse<FILL> (fill pass)",
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "fill_ms": statistics.mean(fill_ms)},
-        "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": nat * 3 * 8,
-                "d2h_bytes_per_step": npairs * BYTES_PER_PAIR,
-                "ms_per_step": 1e3 * statistics.mean(e2e_times)},
+        "e2e": ({"value": e2e_value, "unit": UNIT,
+                 "h2d_bytes_per_step": nat * 3 * 8,
+                 "d2h_bytes_per_step": npairs * BYTES_PER_PAIR,
+                 "ms_per_step": 1e3 * statistics.mean(e2e_times)}
+                if e2e_value is not None else None),
         "gpu_launches": launches,
         "clocks": clk,
-        "fp64_plain": {"value": npairs / (statistics.mean(step64) * 1e-3),
-                       "ms_per_step": statistics.mean(step64),
-                       "fill_ms": statistics.mean(fill64)},
+        "fp64_plain": ({"value": npairs / (statistics.mean(step64) * 1e-3),
+                        "ms_per_step": statistics.mean(step64),
+                        "fill_ms": statistics.mean(fill64)} if step64 else None),
         "stage_ms": {"count_phase": statistics.mean(a - b for a, b in zip(step_ms, fill_ms)),
                      "fill": statistics.mean(fill_ms)},
     }
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and args.reps == 64:
         out["cpu_baseline"] = cpu_baseline()
     print(json.dumps(out), flush=True)
     if dist is not None:

@@ -220,7 +220,10 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_home = L.add(sizeof(HomeCell) * N);
     size_t o_cnt = L.add(sizeof(int32_t) * (N + 1));
     size_t o_off = L.add(sizeof(int64_t) * (N + 1));
-    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err
+    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err, overflow, mask cursor
+    const int64_t mask_cap = std::max<int64_t>(int64_t(1) << 20, 16 * N);
+    size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
+    size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
     if (st != NBL_SUCCESS) return st;
     char *base = static_cast<char *>(p.ws.base);
@@ -254,6 +257,9 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     B.counts = (int32_t *)at(o_cnt);
     B.offsets = (int64_t *)at(o_off);
     B.small = (int *)at(o_small);
+    B.mask_pool = (uint32_t *)at(o_mask);
+    B.mask_cap = mask_cap;
+    B.home_mask = (long long *)at(o_hmask);
     return NBL_SUCCESS;
 }
 
@@ -318,7 +324,7 @@ nbl_status finish_batch(Batch &b, int grid_req) {
 static int traverse_grid(const Plan &p, int64_t natoms) {
     // Persistent-style grid: a few resident CTAs per SM, capped by the number
     // of possible home cells.
-    const int64_t g = std::min<int64_t>((int64_t)p.num_sms * 6, std::max<int64_t>(natoms, 1));
+    const int64_t g = std::min<int64_t>((int64_t)p.num_sms * 8, std::max<int64_t>(natoms, 1));
     return (int)g;
 }
 
@@ -454,9 +460,15 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     ta.pt64 = B.pt64;
     ta.counts = B.counts;
     ta.offsets = B.offsets;
+    ta.mask_pool = B.mask_pool;
+    ta.mask_cursor = reinterpret_cast<unsigned long long *>(B.small + 4);
+    ta.mask_cap = B.mask_cap;
+    ta.home_mask = B.home_mask;
     ta.err = err;
     p.trav_grid = traverse_grid(p, N);
-    NBL_CUDA(launch_traverse(kModeCount, b.fp32, ta, p.trav_grid, st), "count pass");
+    p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
+    NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st),
+             "count pass");
     NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
 
     if (sync) {
@@ -490,7 +502,8 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     ta.shift = o.shift;
     ta.capacity = capacity;
     if (!(o.first || o.second || o.distvec || o.absdist || o.shift)) return NBL_SUCCESS;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, ta, p.trav_grid, st), "fill pass");
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.trav_grid, st),
+             "fill pass");
     return NBL_SUCCESS;
 }
 
@@ -751,7 +764,8 @@ nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
     ta.mat_count = count;
     ta.mat_overflow = p.bufs.small + 2;
     ta.capacity = 0;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, ta, p.trav_grid, st), "matrix fill");
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.trav_grid, st),
+             "matrix fill");
     NBL_CUDA(cudaMemcpyAsync(p.host_small + 2, p.bufs.small + 2, sizeof(int),
                              cudaMemcpyDeviceToHost, st), "read overflow");
     nbl_status r = read_flags(p, st);

@@ -25,6 +25,7 @@
 // count, and in the fill pass the hits go into a per-warp queue that is
 // drained 32 pairs at a time so that the FP64 epilogue and the stores run
 // with full warps and near-contiguous addresses.
+#include <climits>
 #include <cstdint>
 #include <type_traits>
 
@@ -227,49 +228,125 @@ k_gather(GatherArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_traverse: the count and fill passes
+// The pair passes: k_count and k_fill
 // ---------------------------------------------------------------------------
+//
+// Both take one occupied home cell per WARP (warp-strided over the work list;
+// a CTA is four independent warps, so there is no block-wide barrier).  Per
+// home cell, one lane per visited neighbour offset computes the offset vector
+// (FP64, reference order), the wrap counts and the cell slice, and a warp scan
+// turns slice lengths into candidate positions (the "segment batch").
+//
+// k_count stages the candidates in shared memory as FP32 positions in the
+// home-cell frame and sweeps them against the home cell's atoms, four atoms
+// per pass (independent FMA chains), 32 candidates per __ballot_sync.  Each
+// chunk's hit mask is popc'ed into the atom's count and, when the home cell
+// fits the mask pool, stored as one 32-bit word per (atom, chunk).
+//
+// k_fill turns hit words back into pairs lane-parallel: for a window of atoms
+// it builds the prefix of the words' popcounts, then lane L of each round takes
+// output position P = P0 + L, finds its word by binary search and its bit by an
+// n-th-set-bit search, and emits the pair at row_start + rank with exact FP64
+// D, d and S.  Consecutive lanes write consecutive slots.  Home cells without
+// pool words (pool full, more than one segment batch) recompute the words with
+// the same sweep first.
 namespace {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSegBatch = 128;
-constexpr int kITile = 64;
-constexpr int kQueue = 64;
+constexpr int kSeg = 32;         // visited offsets per batch (one per lane)
+constexpr int kITile = 32;       // atoms i per i-tile
+constexpr int kGroup = 4;        // atoms swept together in the FP32 count
+constexpr int kWinWords = 256;   // hit words per emission window
+constexpr int kRange = kWinWords * 32;  // candidates per emission range
+constexpr float kFarCand = 1.0e18f;     // padding candidate
+constexpr float kFarAtom = -1.0e18f;    // padding atom (never near a padding candidate)
 
 template <bool FP32>
-struct TileCfg {
-    static constexpr int kCand = FP32 ? 1024 : 512;
+using CandT = typename std::conditional<FP32, float4, double4>::type;
+
+template <bool FP32>
+struct CountTile {
+    static constexpr int kCand = FP32 ? 256 : 128;
+};
+template <bool FP32>
+struct FillTile {
+    static constexpr int kCand = FP32 ? 64 : 32;
+};
+
+struct SegSmem {
+    double off[kSeg][3];
+    int32_t m[kSeg][3];
+    int32_t b[kSeg];
+    int32_t pref[kSeg + 1];
 };
 
 template <bool FP32>
-struct __align__(16) TravSmem {
-    // segments (visited neighbour cells) of the current batch
-    double seg_off[kSegBatch][3];
-    int32_t seg_m[kSegBatch][3];
-    int32_t seg_b[kSegBatch];
-    int32_t seg_pref[kSegBatch + 1];
-    uint8_t seg_zero[kSegBatch];
-    // candidates of the current tile
-    typename std::conditional<FP32, float4, double4>::type cand[TileCfg<FP32>::kCand];
-    int32_t cand_sj[TileCfg<FP32>::kCand];
-    uint8_t cand_seg[TileCfg<FP32>::kCand];
-    // atoms i of the current i-tile
+struct __align__(16) CountSmem {
+    SegSmem sg;
+    CandT<FP32> cand[CountTile<FP32>::kCand];
+    float4 i32[kITile];
+    int32_t iatom[kITile];
+    int32_t icount[kITile];
+};
+
+constexpr int kChunkSeg = 256;   // chunk -> first segment table (fill)
+
+template <bool FP32>
+struct __align__(16) FillSmem {
+    SegSmem sg;
+    CandT<FP32> cand[FillTile<FP32>::kCand];
     double4 i64[kITile];
     float4 i32[kITile];
     int4 iaux[kITile];
-    long long istate[kITile];  // count (COUNT) or write cursor (FILL)
-    long long istart[kITile];  // row start (FILL)
-    // per-warp emit queue (FILL)
-    int32_t q[kWarps][kQueue];
-    long long qw[kWarps][kQueue];
-    int32_t scan_warp[33];
-    SysDev sys;
+    long long icur[kITile];
+    uint32_t mw[kWinWords];
+    int32_t mpre[kWinWords + 1];
+    uint8_t chunk_seg[kChunkSeg];   // segment of candidate 32*c of the batch
 };
 
-struct Thresh {
+// Per-home-cell constants kept in registers.
+struct Hot {
     float lo_rc, hi_rc, band;
+    double cutoff_sq;
+    int pbc_bits;
+    int ncut;
+    int pt_base;
+    int64_t atom_base;
 };
+
+struct Home {
+    HomeCell hc;
+    const SysDev *S;
+    int2 hs;
+    Hot H;
+    int nvisit;
+};
+
+template <bool FP32>
+__device__ __forceinline__ Home load_home(const TraverseArgs &a, int h) {
+    Home c;
+    c.hc = a.home[h];
+    c.S = a.sys + c.hc.sys;
+    const SysDev &S = *c.S;
+    c.hs = a.table[c.hc.tidx];
+    c.H.lo_rc = c.H.hi_rc = c.H.band = 0.f;
+    if (FP32) {
+        const double R = S.cutoff;
+        const double M = 2.0 * (double)a.amax[c.hc.sys] + S.off_max;
+        const double band = guard_band(M, R);
+        c.H.lo_rc = __double2float_rd(S.cutoff_sq - band);
+        c.H.hi_rc = __double2float_ru(S.cutoff_sq + band);
+        c.H.band = __double2float_ru(band);
+    }
+    c.H.cutoff_sq = S.cutoff_sq;
+    c.H.pbc_bits = (S.pbc[0] ? 1 : 0) | (S.pbc[1] ? 2 : 0) | (S.pbc[2] ? 4 : 0);
+    c.H.ncut = S.ncutoffs;
+    c.H.pt_base = S.pt_base;
+    c.H.atom_base = S.atom_base;
+    c.nvisit = S.nvisit;
+    return c;
+}
 
 __device__ __forceinline__ int2 cell_lookup(const TraverseArgs &a, const SysDev &S,
                                             int sysid, int32_t c0, int32_t c1,
@@ -282,8 +359,115 @@ __device__ __forceinline__ int2 cell_lookup(const TraverseArgs &a, const SysDev 
     return hash_find(a.hkey, a.hmask, a.table, key, a.err);
 }
 
+// Segment batch vb of a home cell: one lane per visited offset
+// (neighbour_visit.hh:63-84).  Returns the batch size, its candidate total
+// and the index of the zero-offset segment (-1 if not in this batch).
+__device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &a,
+                                               const Home &c, int vb, int lane, int &nseg,
+                                               int &total, int &zs) {
+    const unsigned full = 0xffffffffu;
+    const SysDev &S = *c.S;
+    const int nx = S.nscan[0], ny = S.nscan[1], nz = S.nscan[2];
+    const int wx = 2 * nx + 1, wy = 2 * ny + 1;
+    nseg = min(kSeg, c.nvisit - vb);
+    int len = 0;
+    bool zero = false;
+    if (lane < nseg) {
+        const int v = vb + lane;
+        const int xr = v % wx, rest = v / wx;
+        const int yr = rest % wy, zr = rest / wy;
+        const int off3[3] = {xr - nx, yr - ny, zr - nz};
+        int32_t cj[3], m[3];
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            int32_t x = c.hc.c[k] + off3[k];
+            m[k] = 0;
+            if (S.pbc[k]) {
+                m[k] = floor_div(x, S.n[k]);
+                x -= m[k] * S.n[k];
+            } else if (x < 0 || x >= S.n[k]) {
+                ok = false;
+            }
+            cj[k] = x;
+        }
+        int2 sl = make_int2(0, 0);
+        if (ok) sl = cell_lookup(a, S, c.hc.sys, cj[0], cj[1], cj[2]);
+        len = sl.y - sl.x;
+        sg.b[lane] = sl.x;
+        // neighbour_visit.hh:67,73,80: off3 = z b3; off2 = off3 + y b2; off = off2 + x b1
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            double o = dmul((double)off3[2], S.bin[2][k]);
+            o = dadd(o, dmul((double)off3[1], S.bin[1][k]));
+            o = dadd(o, dmul((double)off3[0], S.bin[0][k]));
+            sg.off[lane][k] = o;
+            sg.m[lane][k] = m[k];
+        }
+        zero = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
+    }
+    int incl = len;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(full, incl, d);
+        if (lane >= d) incl += o;
+    }
+    total = __shfl_sync(full, incl, 31);
+    if (lane < nseg) sg.pref[lane] = incl - len;
+    if (lane == 0) sg.pref[nseg] = total;
+    const unsigned zm = __ballot_sync(full, zero);
+    zs = zm ? __ffs(zm) - 1 : -1;
+    __syncwarp();
+}
+
+// Segment of candidate kk of the current batch.
+__device__ __forceinline__ int seg_of(const SegSmem &sg, int nseg, int kk) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sg.pref[mid] <= kk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Stage candidates kb .. kb+nk of the batch, padded to nkp with far points.
+template <bool FP32>
+__device__ __forceinline__ void stage(CandT<FP32> *cand, const SegSmem &sg,
+                                      const TraverseArgs &a, int nseg, int kb, int nk,
+                                      int nkp, int lane) {
+    __syncwarp();
+    for (int k = lane; k < nkp; k += 32) {
+        if (k < nk) {
+            const int kk = kb + k;
+            const int seg = seg_of(sg, nseg, kk);
+            const int sj = sg.b[seg] + (kk - sg.pref[seg]);
+            if constexpr (FP32) {
+                const float4 p = a.pos32[sj];
+                float4 cv;
+                cv.x = p.x + __double2float_rn(sg.off[seg][0]);
+                cv.y = p.y + __double2float_rn(sg.off[seg][1]);
+                cv.z = p.z + __double2float_rn(sg.off[seg][2]);
+                cv.w = p.w;
+                cand[k] = cv;
+            } else {
+                cand[k] = a.pos64[sj];
+            }
+        } else {
+            if constexpr (FP32)
+                cand[k] = make_float4(kFarCand, kFarCand, kFarCand, 0.f);
+            else
+                cand[k] = make_double4(kFarCand, kFarCand, kFarCand, 0.0);
+        }
+    }
+    __syncwarp();
+}
+
 // The reference's exact FP64 inclusion test (neighbour_visit.hh:88-109).
-__device__ __forceinline__ bool exact_inside(const SysDev &S, const TraverseArgs &a,
+template <int KIND>
+__device__ __forceinline__ bool exact_inside(const Hot &H, const TraverseArgs &a,
                                              const double4 &pi, const double4 &pj,
                                              const double *off, float ti_bits,
                                              float tj_bits) {
@@ -291,338 +475,505 @@ __device__ __forceinline__ bool exact_inside(const SysDev &S, const TraverseArgs
     const double dy = dadd(dsub(pj.y, pi.y), off[1]);
     const double dz = dadd(dsub(pj.z, pi.z), off[2]);
     const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-    if (!(r2 < S.cutoff_sq)) return false;
-    if (S.cutoff_kind == kCutPerAtom) {
+    if (!(r2 < H.cutoff_sq)) return false;
+    if (KIND == kCutPerAtom) {
         const double cc = dadd(pi.w, pj.w);
         return r2 < dmul(cc, cc);
     }
-    if (S.cutoff_kind == kCutPerType) {
+    if (KIND == kCutPerType) {
         const int ti = __float_as_int(ti_bits), tj = __float_as_int(tj_bits);
-        if (ti >= 0 && ti < S.ncutoffs && tj >= 0 && tj < S.ncutoffs)
-            return r2 < a.pt64[S.pt_base + ti * S.ncutoffs + tj];
+        if (ti >= 0 && ti < H.ncut && tj >= 0 && tj < H.ncut)
+            return r2 < a.pt64[H.pt_base + ti * H.ncut + tj];
     }
     return true;
 }
 
-template <bool FP32>
-__device__ __forceinline__ void pair_threshold(const SysDev &S, const TraverseArgs &a,
-                                               const Thresh &th, float wi, float wj,
-                                               float &lo, float &hi) {
-    lo = th.lo_rc;
-    hi = th.hi_rc;
-    if (S.cutoff_kind == kCutPerAtom) {
+// Guard-band candidate kk of the batch for atom si, decided in FP64 (cold).
+template <int KIND>
+__device__ __noinline__ bool resolve_exact(const SegSmem &sg, const TraverseArgs &a,
+                                           const Hot &H, int nseg, int kk, int si,
+                                           float wi) {
+    const int seg = seg_of(sg, nseg, kk);
+    const int32_t sj = sg.b[seg] + (kk - sg.pref[seg]);
+    return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], sg.off[seg], wi,
+                              a.pos32[sj].w);
+}
+
+// FP32 thresholds for one (atom, candidate) pair.
+template <int KIND>
+__device__ __forceinline__ void thresholds(const Hot &H, const TraverseArgs &a, float wi,
+                                           float wj, float &lo, float &hi) {
+    lo = H.lo_rc;
+    hi = H.hi_rc;
+    if (KIND == kCutPerAtom) {
         const float cc = wi + wj;
         const float t = cc * cc;
-        lo = fminf(lo, t - th.band);
-        hi = fminf(hi, t + th.band);
-    } else if (S.cutoff_kind == kCutPerType) {
+        lo = fminf(lo, t - H.band);
+        hi = fminf(hi, t + H.band);
+    } else if (KIND == kCutPerType) {
         const int ti = __float_as_int(wi), tj = __float_as_int(wj);
-        if (ti >= 0 && ti < S.ncutoffs && tj >= 0 && tj < S.ncutoffs) {
-            const float t = a.pt32[S.pt_base + ti * S.ncutoffs + tj];
-            lo = fminf(lo, t - th.band);
-            hi = fminf(hi, t + th.band);
+        if (ti >= 0 && ti < H.ncut && tj >= 0 && tj < H.ncut) {
+            const float t = a.pt32[H.pt_base + ti * H.ncut + tj];
+            lo = fminf(lo, t - H.band);
+            hi = fminf(hi, t + H.band);
         }
     }
 }
 
-// Emit up to 32 queued pairs (lane L takes entry L).
-template <bool FP32>
-__device__ __forceinline__ void emit_queue(TravSmem<FP32> &sm, const TraverseArgs &a,
-                                           const SysDev &S, int warp, int lane,
-                                           int count) {
-    if (lane < count) {
-        const int32_t e = sm.q[warp][lane];
-        const long long slot = sm.qw[warp][lane];
-        const int k = e & 0xffff, il = e >> 16;
-        const int32_t sj = sm.cand_sj[k];
-        const int seg = sm.cand_seg[k];
-        const double4 pj = a.pos64[sj];
-        const double4 pi = sm.i64[il];
-        const int4 aj = a.aux[sj];
-        const int4 ai = sm.iaux[il];
-        const double dx = dadd(dsub(pj.x, pi.x), sm.seg_off[seg][0]);
-        const double dy = dadd(dsub(pj.y, pi.y), sm.seg_off[seg][1]);
-        const double dz = dadd(dsub(pj.z, pi.z), sm.seg_off[seg][2]);
-        if (a.mat_k > 0) {
-            const long long sl = slot - sm.istart[il];
-            if (sl < a.mat_k) {
-                const long long m = (long long)ai.x * a.mat_k + sl;
-                a.mat_idx[m] = (int32_t)(aj.x - S.atom_base);
-                a.mat_dist[3 * m + 0] = dx;
-                a.mat_dist[3 * m + 1] = dy;
-                a.mat_dist[3 * m + 2] = dz;
-            }
-        } else if (slot < a.capacity) {
-            const int32_t il_out = (int32_t)(ai.x - S.atom_base);
-            const int32_t jl_out = (int32_t)(aj.x - S.atom_base);
-            if (a.first) a.first[slot] = il_out;
-            if (a.second) a.second[slot] = jl_out;
-            if (a.distvec) {
-                a.distvec[3 * slot + 0] = dx;
-                a.distvec[3 * slot + 1] = dy;
-                a.distvec[3 * slot + 2] = dz;
-            }
-            if (a.absdist) {
-                const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-                a.absdist[slot] = __dsqrt_rn(r2);
-            }
-            if (a.shift) {
-                a.shift[3 * slot + 0] = ai.y - (S.pbc[0] ? aj.y : 0) + sm.seg_m[seg][0];
-                a.shift[3 * slot + 1] = ai.z - (S.pbc[1] ? aj.z : 0) + sm.seg_m[seg][1];
-                a.shift[3 * slot + 2] = ai.w - (S.pbc[2] ? aj.w : 0) + sm.seg_m[seg][2];
-            }
+// Hit mask of one staged 32-candidate chunk (tile positions k0..k0+31) for one
+// atom: FP32 filter + FP64 guard band, or plain FP64.
+template <bool FP32, int KIND>
+__device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const SegSmem &sg,
+                                               const TraverseArgs &a, const Hot &H,
+                                               int nseg, int kb, int k0, int lane,
+                                               int kself_tile, int si, const float4 &pi32,
+                                               const double4 &pi64) {
+    const unsigned full = 0xffffffffu;
+    const int k = k0 + lane;
+    const bool notself = k != kself_tile;
+    if constexpr (FP32) {
+        const float4 cv = cand[k];
+        const float dx = cv.x - pi32.x;
+        const float dy = cv.y - pi32.y;
+        const float dz = cv.z - pi32.z;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        float lo, hi;
+        thresholds<KIND>(H, a, pi32.w, cv.w, lo, hi);
+        unsigned mask = __ballot_sync(full, (r2 < lo) && notself);
+        const bool amb = !(r2 < lo) && (r2 < hi) && notself;
+        if (__any_sync(full, amb)) {
+            bool h2 = false;
+            if (amb) h2 = resolve_exact<KIND>(sg, a, H, nseg, kb + k, si, pi32.w);
+            mask |= __ballot_sync(full, h2);
+        }
+        return mask;
+    } else {
+        bool hit = false;
+        const double4 pj = cand[k];
+        if (notself && pj.x != (double)kFarCand) {
+            const int seg = seg_of(sg, nseg, kb + k);
+            float tj = 0.f;
+            if (KIND == kCutPerType) tj = a.pos32[sg.b[seg] + (kb + k - sg.pref[seg])].w;
+            hit = exact_inside<KIND>(H, a, pi64, pj, sg.off[seg], pi32.w, tj);
+        }
+        return __ballot_sync(full, hit);
+    }
+}
+
+// Position of the (r+1)-th set bit of w (r < popc(w)).
+__device__ __forceinline__ int nth_set_bit(unsigned w, int r) {
+    int pos = 0;
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        const unsigned low = w & ((1u << sh) - 1u);
+        const int c = __popc(low);
+        if (r >= c) {
+            r -= c;
+            w >>= sh;
+            pos += sh;
         } else {
-            atomicOr(a.err, kErrCapacity);
+            w = low;
         }
     }
+    return pos;
+}
+
+// w / n for 0 <= w < 2^20 and small n, without an integer division.
+__device__ __forceinline__ int div_small(int w, int n, float inv_n) {
+    int q = __float2int_rz((float)w * inv_n);
+    if (q * n > w) q--;
+    if ((q + 1) * n <= w) q++;
+    return q;
 }
 
 }  // namespace
 
-template <int MODE, bool FP32>
-__global__ void __launch_bounds__(kThreads)
-k_traverse(TraverseArgs a) {
-    constexpr int kCand = TileCfg<FP32>::kCand;
-    __shared__ TravSmem<FP32> sm;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+template <bool FP32, int KIND>
+__global__ void __launch_bounds__(kThreads, 6)
+k_count(TraverseArgs a) {
+    constexpr int kCand = CountTile<FP32>::kCand;
+    __shared__ CountSmem<FP32> smem[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CountSmem<FP32> &sm = smem[warp];
     const unsigned full = 0xffffffffu;
     const int nhome = *a.n_home;
+    const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    for (int h = blockIdx.x; h < nhome; h += gridDim.x) {
-        const HomeCell hc = a.home[h];
-        // System descriptor -> shared memory (broadcast reads in the sweep).
-        {
-            const int *src = reinterpret_cast<const int *>(a.sys + hc.sys);
-            int *dst = reinterpret_cast<int *>(&sm.sys);
-            for (int w = tid; w < (int)(sizeof(SysDev) / sizeof(int)); w += kThreads)
-                dst[w] = src[w];
-        }
-        __syncthreads();
-        const SysDev &S = sm.sys;
-        const int2 hs = a.table[hc.tidx];
-        Thresh th;
-        if (FP32) {
-            const double R = S.cutoff;
-            const double M = 2.0 * (double)a.amax[hc.sys] + S.off_max;
-            const double band = guard_band(M, R);
-            th.lo_rc = __double2float_rd(S.cutoff_sq - band);
-            th.hi_rc = __double2float_ru(S.cutoff_sq + band);
-            th.band = __double2float_ru(band);
-        }
-        const int nx = S.nscan[0], ny = S.nscan[1], nz = S.nscan[2];
-        const int wx = 2 * nx + 1, wy = 2 * ny + 1;
+    for (int h = gwarp; h < nhome; h += nwarps) {
+        const Home c = load_home<FP32>(a, h);
+        const Hot &H = c.H;
+        const int2 hs = c.hs;
+        const bool one_batch = c.nvisit <= kSeg;
+        long long mbase = -1;
 
         for (int ib = hs.x; ib < hs.y; ib += kITile) {
             const int ni = min(kITile, hs.y - ib);
-            if (tid < ni) {
-                const int si = ib + tid;
-                sm.i64[tid] = a.pos64[si];
-                sm.i32[tid] = a.pos32[si];
-                const int4 ax = a.aux[si];
-                sm.iaux[tid] = ax;
-                sm.istate[tid] = (MODE == kModeCount) ? 0ll : (long long)a.offsets[ax.x];
-                if (MODE == kModeFill) sm.istart[tid] = sm.istate[tid];
+            if (lane < ni) {
+                sm.i32[lane] = a.pos32[ib + lane];
+                sm.iatom[lane] = a.aux[ib + lane].x;
+                sm.icount[lane] = 0;
             }
-            __syncthreads();
-
-            for (int vb = 0; vb < S.nvisit; vb += kSegBatch) {
-                const int nseg = min(kSegBatch, S.nvisit - vb);
-                // --- segment set-up: one thread per visited offset -----------
-                int len = 0;
-                if (tid < nseg) {
-                    const int v = vb + tid;
-                    const int xr = v % wx, rest = v / wx;
-                    const int yr = rest % wy, zr = rest / wy;
-                    const int off3[3] = {xr - nx, yr - ny, zr - nz};
-                    int32_t cj[3], m[3];
-                    bool ok = true;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        int32_t x = hc.c[k] + off3[k];
-                        m[k] = 0;
-                        if (S.pbc[k]) {
-                            m[k] = floor_div(x, S.n[k]);
-                            x -= m[k] * S.n[k];
-                        } else if (x < 0 || x >= S.n[k]) {
-                            ok = false;
-                        }
-                        cj[k] = x;
+            for (int vb = 0; vb < c.nvisit; vb += kSeg) {
+                int nseg, total, zs;
+                setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
+                const int nchunks_all = (total + 31) >> 5;
+                // One word region per home cell, taken with its first i-tile:
+                // (atoms of the cell) x (chunks of the candidate list).
+                if (ib == hs.x && vb == 0 && a.mask_pool != nullptr) {
+                    long long base = -1;
+                    if (lane == 0 && one_batch && nchunks_all <= kWinWords) {
+                        const long long words = (long long)(hs.y - hs.x) * nchunks_all;
+                        const unsigned long long b =
+                            atomicAdd(a.mask_cursor, (unsigned long long)words);
+                        if ((long long)b + words <= a.mask_cap) base = (long long)b;
                     }
-                    int2 sl = make_int2(0, 0);
-                    if (ok) sl = cell_lookup(a, S, hc.sys, cj[0], cj[1], cj[2]);
-                    len = sl.y - sl.x;
-                    sm.seg_b[tid] = sl.x;
-                    // neighbour_visit.hh:67,73,80: off3 = z b3; off2 = off3 + y b2;
-                    // off = off2 + x b1
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        double o = dmul((double)off3[2], S.bin[2][k]);
-                        o = dadd(o, dmul((double)off3[1], S.bin[1][k]));
-                        o = dadd(o, dmul((double)off3[0], S.bin[0][k]));
-                        sm.seg_off[tid][k] = o;
-                        sm.seg_m[tid][k] = m[k];
-                    }
-                    sm.seg_zero[tid] = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
+                    base = __shfl_sync(full, base, 0);
+                    if (lane == 0) a.home_mask[h] = base;
+                    mbase = base;
                 }
-                // block-wide exclusive scan of the segment lengths
-                {
-                    int incl = len;
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        int o = __shfl_up_sync(full, incl, d);
-                        if (lane >= d) incl += o;
-                    }
-                    if (lane == 31) sm.scan_warp[warp] = incl;
-                    __syncthreads();
-                    int wbase = 0, tot = 0;
-#pragma unroll
-                    for (int w = 0; w < kWarps; w++) {
-                        const int ws = sm.scan_warp[w];
-                        if (w < warp) wbase += ws;
-                        tot += ws;
-                    }
-                    if (tid < nseg) sm.seg_pref[tid] = wbase + incl - len;
-                    if (tid == 0) sm.seg_pref[nseg] = tot;
-                    __syncthreads();
-                }
-                const int total = sm.seg_pref[nseg];
+                // candidate index of atom si itself at offset 0 is kself0 + si
+                const int kself0 = (zs >= 0) ? sm.sg.pref[zs] - sm.sg.b[zs] : INT_MIN / 2;
 
                 for (int kb = 0; kb < total; kb += kCand) {
                     const int nk = min(kCand, total - kb);
-                    // --- stage candidates ------------------------------------
-                    for (int k = tid; k < nk; k += kThreads) {
-                        const int kk = kb + k;
-                        int lo = 0, hi = nseg - 1;  // last seg with pref <= kk
-                        while (lo < hi) {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (sm.seg_pref[mid] <= kk)
-                                lo = mid;
-                            else
-                                hi = mid - 1;
-                        }
-                        const int sj = sm.seg_b[lo] + (kk - sm.seg_pref[lo]);
-                        if (FP32) {
-                            const float4 p = a.pos32[sj];
-                            float4 cv;
-                            cv.x = p.x + __double2float_rn(sm.seg_off[lo][0]);
-                            cv.y = p.y + __double2float_rn(sm.seg_off[lo][1]);
-                            cv.z = p.z + __double2float_rn(sm.seg_off[lo][2]);
-                            cv.w = p.w;
-                            reinterpret_cast<float4 *>(sm.cand)[k] = cv;
-                        } else {
-                            reinterpret_cast<double4 *>(sm.cand)[k] = a.pos64[sj];
-                        }
-                        sm.cand_sj[k] = sj;
-                        sm.cand_seg[k] = (uint8_t)lo;
-                    }
-                    __syncthreads();
-
-                    // --- sweep: warp per atom i ------------------------------
-                    int qn = 0;  // warp-uniform queue length (FILL)
-                    for (int il = warp; il < ni; il += kWarps) {
-                        const int si = ib + il;
-                        const float4 pi32 = sm.i32[il];
-                        const double4 pi64 = sm.i64[il];
-                        long long state = sm.istate[il];
-                        for (int k0 = 0; k0 < nk; k0 += 32) {
-                            const int k = k0 + lane;
-                            bool hit = false;
-                            if (k < nk) {
-                                const int seg = sm.cand_seg[k];
-                                const bool self =
-                                    (sm.cand_sj[k] == si) && sm.seg_zero[seg];
-                                if (!self) {
-                                    if (FP32) {
-                                        const float4 cv = reinterpret_cast<const float4 *>(sm.cand)[k];
-                                        const float dx = cv.x - pi32.x;
-                                        const float dy = cv.y - pi32.y;
-                                        const float dz = cv.z - pi32.z;
-                                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                                        float lo, hi;
-                                        pair_threshold<FP32>(S, a, th, pi32.w, cv.w, lo, hi);
-                                        if (r2 < lo) {
-                                            hit = true;
-                                        } else if (r2 < hi) {
-                                            const double4 pj = a.pos64[sm.cand_sj[k]];
-                                            const float wj = a.pos32[sm.cand_sj[k]].w;
-                                            hit = exact_inside(S, a, pi64, pj, sm.seg_off[seg],
-                                                               pi32.w, wj);
-                                        }
-                                    } else {
-                                        const double4 pj = reinterpret_cast<const double4 *>(sm.cand)[k];
-                                        float wj = 0.f;
-                                        if (S.cutoff_kind == kCutPerType)
-                                            wj = a.pos32[sm.cand_sj[k]].w;
-                                        hit = exact_inside(S, a, pi64, pj, sm.seg_off[seg],
-                                                           pi32.w, wj);
+                    const int nkp = (nk + 31) & ~31;
+                    const int nck = nkp >> 5;
+                    stage<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
+                    if constexpr (FP32) {
+                        // kGroup atoms per pass over the tile
+                        for (int g0 = 0; g0 < ni; g0 += kGroup) {
+                            float4 pg[kGroup];
+                            int ks[kGroup], cnt[kGroup];
+                            unsigned mw[kGroup];
+#pragma unroll
+                            for (int g = 0; g < kGroup; g++) {
+                                const bool v = g0 + g < ni;
+                                pg[g] = v ? sm.i32[g0 + g]
+                                          : make_float4(kFarAtom, kFarAtom, kFarAtom, 0.f);
+                                ks[g] = v ? kself0 + (ib + g0 + g) - kb : -1;
+                                cnt[g] = 0;
+                                mw[g] = 0u;
+                            }
+                            for (int ch = 0; ch < nck; ch++) {
+                                const int k = ch * 32 + lane;
+                                const float4 cv = sm.cand[k];
+                                unsigned m[kGroup];
+                                bool amb_any = false, amb[kGroup];
+#pragma unroll
+                                for (int g = 0; g < kGroup; g++) {
+                                    const float dx = cv.x - pg[g].x;
+                                    const float dy = cv.y - pg[g].y;
+                                    const float dz = cv.z - pg[g].z;
+                                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                                    float lo, hi;
+                                    thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
+                                    const bool notself = k != ks[g];
+                                    m[g] = __ballot_sync(full, (r2 < lo) && notself);
+                                    amb[g] = !(r2 < lo) && (r2 < hi) && notself;
+                                    amb_any |= amb[g];
+                                }
+                                if (__any_sync(full, amb_any)) {
+#pragma unroll
+                                    for (int g = 0; g < kGroup; g++) {
+                                        bool h2 = false;
+                                        if (amb[g])
+                                            h2 = resolve_exact<KIND>(sm.sg, a, H, nseg, kb + k,
+                                                                     ib + g0 + g, pg[g].w);
+                                        m[g] |= __ballot_sync(full, h2);
+                                    }
+                                }
+                                const bool mine = lane == (ch & 31);
+#pragma unroll
+                                for (int g = 0; g < kGroup; g++) {
+                                    cnt[g] += __popc(m[g]);
+                                    mw[g] = mine ? m[g] : mw[g];
+                                }
+                                if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
+                                    const long long w0 = mbase + (kb >> 5) + (ch & ~31) + lane;
+#pragma unroll
+                                    for (int g = 0; g < kGroup; g++) {
+                                        if (g0 + g < ni && lane <= (ch & 31))
+                                            a.mask_pool[w0 + (long long)(ib + g0 + g - hs.x) *
+                                                                 nchunks_all] = mw[g];
                                     }
                                 }
                             }
-                            const unsigned mask = __ballot_sync(full, hit);
-                            if (MODE == kModeCount) {
-                                state += __popc(mask);
-                            } else if (mask) {
-                                const int before = __popc(mask & lanemask_lt());
-                                if (hit) {
-                                    sm.q[warp][qn + before] = k | (il << 16);
-                                    sm.qw[warp][qn + before] = state + before;
-                                }
-                                state += __popc(mask);
-                                qn += __popc(mask);
-                                __syncwarp();
-                                if (qn >= 32) {
-                                    emit_queue<FP32>(sm, a, S, warp, lane, 32);
-                                    __syncwarp();
-                                    const int rem = qn - 32;
-                                    int32_t e = 0;
-                                    long long w = 0;
-                                    if (lane < rem) {
-                                        e = sm.q[warp][32 + lane];
-                                        w = sm.qw[warp][32 + lane];
-                                    }
-                                    __syncwarp();
-                                    if (lane < rem) {
-                                        sm.q[warp][lane] = e;
-                                        sm.qw[warp][lane] = w;
-                                    }
-                                    __syncwarp();
-                                    qn = rem;
+                            if (lane < kGroup && g0 + lane < ni) {
+                                int cg = cnt[0];
+#pragma unroll
+                                for (int g = 1; g < kGroup; g++)
+                                    if (lane == g) cg = cnt[g];
+                                sm.icount[g0 + lane] += cg;
+                            }
+                            __syncwarp();
+                        }
+                    } else {
+                        for (int il = 0; il < ni; il++) {
+                            const int si = ib + il;
+                            const float4 pi32 = sm.i32[il];
+                            const double4 pi64 = a.pos64[si];
+                            const int kself_tile = kself0 + si - kb;
+                            int cnt = 0;
+                            unsigned mword = 0;
+                            for (int ch = 0; ch < nck; ch++) {
+                                const unsigned mask = chunk_mask<FP32, KIND>(
+                                    sm.cand, sm.sg, a, H, nseg, kb, ch * 32, lane, kself_tile,
+                                    si, pi32, pi64);
+                                cnt += __popc(mask);
+                                mword = (lane == (ch & 31)) ? mask : mword;
+                                if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
+                                    if (lane <= (ch & 31))
+                                        a.mask_pool[mbase + (long long)(si - hs.x) * nchunks_all +
+                                                    (kb >> 5) + (ch & ~31) + lane] = mword;
                                 }
                             }
+                            if (lane == 0) sm.icount[il] += cnt;
+                            __syncwarp();
                         }
-                        if (lane == 0) sm.istate[il] = state;
-                    }
-                    if (MODE == kModeFill && qn > 0) {
-                        emit_queue<FP32>(sm, a, S, warp, lane, qn);
-                    }
-                    __syncthreads();
-                }
-            }
-            // --- per-atom results of this i-tile ---------------------------------
-            if (tid < ni) {
-                const int4 ax = sm.iaux[tid];
-                if (MODE == kModeCount) {
-                    a.counts[ax.x] = (int32_t)sm.istate[tid];
-                } else {
-                    const long long end = (long long)a.offsets[ax.x + 1];
-                    if (sm.istate[tid] != end) atomicOr(a.err, kErrInternal);
-                    if (a.mat_k > 0) {
-                        const long long deg = end - sm.istart[tid];
-                        a.mat_count[ax.x] = (int32_t)deg;
-                        if (deg > a.mat_k) atomicOr(a.mat_overflow, 1);
                     }
                 }
             }
-            __syncthreads();
+            if (lane < ni) a.counts[sm.iatom[lane]] = sm.icount[lane];
+            __syncwarp();
         }
-        __syncthreads();
     }
 }
 
-template __global__ void k_traverse<kModeCount, true>(TraverseArgs);
-template __global__ void k_traverse<kModeCount, false>(TraverseArgs);
-template __global__ void k_traverse<kModeFill, true>(TraverseArgs);
-template __global__ void k_traverse<kModeFill, false>(TraverseArgs);
+// Segment of candidate kk, starting from the chunk's first segment.
+template <bool FP32>
+__device__ __forceinline__ int seg_of_fast(const FillSmem<FP32> &sm, int nseg,
+                                           int nchunks, int kk) {
+    const int c = kk >> 5;
+    if (c >= kChunkSeg || c >= nchunks) return seg_of(sm.sg, nseg, kk);
+    int seg = sm.chunk_seg[c];
+    while (seg + 1 < nseg && sm.sg.pref[seg + 1] <= kk) seg++;
+    return seg;
+}
+
+// One output pair in flight: where it goes and the j-side data it needs.
+struct PairWork {
+    bool act;
+    int il, seg;
+    long long slot;
+    double4 pj;
+    int4 aj;
+};
+
+// Map window position P to its pair and issue the j-side loads.
+template <bool FP32>
+__device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
+                                               const TraverseArgs &a, int nseg, int nchunks,
+                                               int nw, int nch, float inv_nch, int kr,
+                                               int a0, int total_w, int P) {
+    PairWork w;
+    w.act = P < total_w;
+    w.il = 0;
+    w.seg = 0;
+    w.slot = 0;
+    if (w.act) {
+        int lo = 0, hi = nw - 1;  // last word with mpre <= P
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sm.mpre[mid] <= P)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int bit = nth_set_bit(sm.mw[lo], P - sm.mpre[lo]);
+        const int al = div_small(lo, nch, inv_nch);
+        const int kk = kr + (lo - al * nch) * 32 + bit;
+        w.il = a0 + al;
+        w.slot = sm.icur[w.il] + (P - sm.mpre[al * nch]);
+        w.seg = seg_of_fast(sm, nseg, nchunks, kk);
+        const int32_t sj = sm.sg.b[w.seg] + (kk - sm.sg.pref[w.seg]);
+        w.pj = a.pos64[sj];
+        w.aj = a.aux[sj];
+    }
+    return w;
+}
+
+// Compute and store one pair (exact FP64 D and d, S, i, j).
+template <bool FP32>
+__device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const TraverseArgs &a,
+                                           const Hot &H, const PairWork &w) {
+    if (!w.act) return;
+    const double4 pi = sm.i64[w.il];
+    const int4 ai = sm.iaux[w.il];
+    const int seg = w.seg;
+    const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
+    const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
+    const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
+    const int32_t jl = (int32_t)(w.aj.x - H.atom_base);
+    if (a.mat_k > 0) {
+        const long long rank = w.slot - (long long)a.offsets[ai.x];
+        if (rank < a.mat_k) {
+            const long long m = (long long)ai.x * a.mat_k + rank;
+            a.mat_idx[m] = jl;
+            a.mat_dist[3 * m + 0] = dx;
+            a.mat_dist[3 * m + 1] = dy;
+            a.mat_dist[3 * m + 2] = dz;
+        }
+        return;
+    }
+    const long long slot = w.slot;
+    if (slot >= a.capacity) {
+        atomicOr(a.err, kErrCapacity);
+        return;
+    }
+    if (a.first) __stcs(a.first + slot, (int32_t)(ai.x - H.atom_base));
+    if (a.second) __stcs(a.second + slot, jl);
+    if (a.absdist) {
+        const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+        __stcs(a.absdist + slot, __dsqrt_rn(r2));
+    }
+    if (a.distvec) {
+        double *D = a.distvec + 3 * slot;
+        D[0] = dx;
+        D[1] = dy;
+        D[2] = dz;
+    }
+    if (a.shift) {
+        int32_t *Sv = a.shift + 3 * slot;
+        Sv[0] = ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0];
+        Sv[1] = ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1];
+        Sv[2] = ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + sm.sg.m[seg][2];
+    }
+}
+
+template <bool FP32, int KIND>
+__global__ void __launch_bounds__(kThreads, 4)
+k_fill(TraverseArgs a) {
+    constexpr int kCand = FillTile<FP32>::kCand;
+    __shared__ FillSmem<FP32> smem[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FillSmem<FP32> &sm = smem[warp];
+    const unsigned full = 0xffffffffu;
+    const int nhome = *a.n_home;
+    const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
+
+    for (int h = gwarp; h < nhome; h += nwarps) {
+        const Home c = load_home<FP32>(a, h);
+        const Hot &H = c.H;
+        const int2 hs = c.hs;
+        const bool one_batch = c.nvisit <= kSeg;
+        const long long mbase =
+            (a.mask_pool != nullptr && one_batch) ? a.home_mask[h] : -1ll;
+
+        for (int ib = hs.x; ib < hs.y; ib += kITile) {
+            const int ni = min(kITile, hs.y - ib);
+            if (lane < ni) {
+                const int si = ib + lane;
+                sm.i32[lane] = a.pos32[si];
+                sm.i64[lane] = a.pos64[si];
+                const int4 ax = a.aux[si];
+                sm.iaux[lane] = ax;
+                sm.icur[lane] = (long long)a.offsets[ax.x];
+            }
+            for (int vb = 0; vb < c.nvisit; vb += kSeg) {
+                int nseg, total, zs;
+                setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
+                const int nchunks = (total + 31) >> 5;
+                for (int cc = lane; cc < nchunks && cc < kChunkSeg; cc += 32)
+                    sm.chunk_seg[cc] = (uint8_t)seg_of(sm.sg, nseg, cc * 32);
+                __syncwarp();
+                const int kself0 = (zs >= 0) ? sm.sg.pref[zs] - sm.sg.b[zs] : INT_MIN / 2;
+
+                for (int kr = 0; kr < total; kr += kRange) {
+                    const int nrange = min(kRange, total - kr);
+                    const int nch = (nrange + 31) >> 5;
+                    const float inv_nch = 1.0f / (float)nch;
+                    const int win = max(1, kWinWords / nch);
+                    for (int a0 = 0; a0 < ni; a0 += win) {
+                        const int na = min(win, ni - a0);
+                        const int nw = na * nch;
+                        // --- the window's hit words ---------------------------------
+                        if (mbase >= 0) {
+                            for (int w = lane; w < nw; w += 32) {
+                                const int al = div_small(w, nch, inv_nch);
+                                sm.mw[w] = a.mask_pool[mbase +
+                                                       (long long)(ib + a0 + al - hs.x) *
+                                                           nchunks + (kr >> 5) + (w - al * nch)];
+                            }
+                        } else {
+                            for (int kt = 0; kt < nrange; kt += kCand) {
+                                const int nk = min(kCand, nrange - kt);
+                                const int nkp = (nk + 31) & ~31;
+                                stage<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
+                                for (int al = 0; al < na; al++) {
+                                    const int il = a0 + al, si = ib + il;
+                                    const float4 pi32 = sm.i32[il];
+                                    const double4 pi64 = sm.i64[il];
+                                    const int kself_tile = kself0 + si - (kr + kt);
+                                    for (int ch = 0; ch < (nkp >> 5); ch++) {
+                                        const unsigned mask = chunk_mask<FP32, KIND>(
+                                            sm.cand, sm.sg, a, H, nseg, kr + kt, ch * 32, lane,
+                                            kself_tile, si, pi32, pi64);
+                                        if (lane == 0) sm.mw[al * nch + (kt >> 5) + ch] = mask;
+                                    }
+                                }
+                            }
+                        }
+                        __syncwarp();
+                        // --- prefix of the words' popcounts ---------------------------
+                        int carry = 0;
+                        for (int w0 = 0; w0 < nw; w0 += 32) {
+                            const int w = w0 + lane;
+                            const int p = (w < nw) ? __popc(sm.mw[w]) : 0;
+                            int incl = p;
+#pragma unroll
+                            for (int d = 1; d < 32; d <<= 1) {
+                                const int o = __shfl_up_sync(full, incl, d);
+                                if (lane >= d) incl += o;
+                            }
+                            if (w < nw) sm.mpre[w] = carry + incl - p;
+                            carry += __shfl_sync(full, incl, 31);
+                        }
+                        if (lane == 0) sm.mpre[nw] = carry;
+                        __syncwarp();
+                        // --- emission, software-pipelined: the next round's j-side
+                        //     loads are in flight while the current round computes ----
+                        PairWork cur = fetch_pair<FP32>(sm, a, nseg, nchunks, nw, nch,
+                                                        inv_nch, kr, a0, carry, lane);
+                        for (int P0 = 0; P0 < carry; P0 += 32) {
+                            const PairWork nxt = fetch_pair<FP32>(sm, a, nseg, nchunks, nw,
+                                                                  nch, inv_nch, kr, a0, carry,
+                                                                  P0 + 32 + lane);
+                            store_pair<FP32>(sm, a, H, cur);
+                            cur = nxt;
+                        }
+                        __syncwarp();
+                        if (lane < na)
+                            sm.icur[a0 + lane] += sm.mpre[(lane + 1) * nch] - sm.mpre[lane * nch];
+                        __syncwarp();
+                    }
+                }
+            }
+            // --- fill must land exactly on the next row; matrix row lengths --------
+            if (lane < ni) {
+                const int ax = sm.iaux[lane].x;
+                const long long end = (long long)a.offsets[ax + 1];
+                if (sm.icur[lane] != end) atomicOr(a.err, kErrInternal);
+                if (a.mat_k > 0) {
+                    const long long deg = end - (long long)a.offsets[ax];
+                    a.mat_count[ax] = (int32_t)deg;
+                    if (deg > a.mat_k) atomicOr(a.mat_overflow, 1);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+#define NBL_INST(F, K)                                            \
+    template __global__ void k_count<F, K>(TraverseArgs);         \
+    template __global__ void k_fill<F, K>(TraverseArgs);
+NBL_INST(true, kCutScalar)
+NBL_INST(true, kCutPerAtom)
+NBL_INST(true, kCutPerType)
+NBL_INST(false, kCutScalar)
+NBL_INST(false, kCutPerAtom)
+NBL_INST(false, kCutPerType)
+#undef NBL_INST
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st) {
     if (a.natoms <= 0) return cudaSuccess;
@@ -640,20 +991,32 @@ cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_traverse(int mode, bool fp32, const TraverseArgs &a, int grid,
-                            cudaStream_t st) {
+cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
+                            int grid, cudaStream_t st) {
     if (grid <= 0) return cudaSuccess;
+#define NBL_GO(KERNEL, F, K) KERNEL<F, K><<<grid, kThreads, 0, st>>>(a)
+#define NBL_BY_KIND(KERNEL, F)                        \
+    do {                                              \
+        if (kind == kCutPerAtom)                      \
+            NBL_GO(KERNEL, F, kCutPerAtom);           \
+        else if (kind == kCutPerType)                 \
+            NBL_GO(KERNEL, F, kCutPerType);           \
+        else                                          \
+            NBL_GO(KERNEL, F, kCutScalar);            \
+    } while (0)
     if (mode == kModeCount) {
         if (fp32)
-            k_traverse<kModeCount, true><<<grid, kThreads, 0, st>>>(a);
+            NBL_BY_KIND(k_count, true);
         else
-            k_traverse<kModeCount, false><<<grid, kThreads, 0, st>>>(a);
+            NBL_BY_KIND(k_count, false);
     } else {
         if (fp32)
-            k_traverse<kModeFill, true><<<grid, kThreads, 0, st>>>(a);
+            NBL_BY_KIND(k_fill, true);
         else
-            k_traverse<kModeFill, false><<<grid, kThreads, 0, st>>>(a);
+            NBL_BY_KIND(k_fill, false);
     }
+#undef NBL_BY_KIND
+#undef NBL_GO
     count_launch();
     return cudaGetLastError();
 }

@@ -71,6 +71,14 @@ struct TraverseArgs {
     // Dense-matrix sink (neighbour_matrix): when mat_k > 0 the fill pass writes
     // row (global atom index) a, slot s < mat_k of mat_idx / mat_dist instead
     // of the pair list, and mat_count[a] = row length.
+    // Hit-mask pool: the count pass stores one 32-bit word per (atom,
+    // 32-candidate chunk) for each home cell it can fit (home_mask[h] = first
+    // word, -1 if none); the fill pass then reads the words instead of
+    // repeating the distance sweep.  mask_pool == nullptr disables it.
+    uint32_t *mask_pool;
+    unsigned long long *mask_cursor;
+    long long mask_cap;
+    long long *home_mask;
     int32_t mat_k;
     int32_t *mat_idx;
     double *mat_dist;
@@ -81,7 +89,7 @@ struct TraverseArgs {
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
-cudaError_t launch_traverse(int mode, bool fp32, const TraverseArgs &a, int grid,
-                            cudaStream_t st);
+cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
+                            int grid, cudaStream_t st);
 
 }  // namespace nbl

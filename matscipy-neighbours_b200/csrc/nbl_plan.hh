@@ -52,7 +52,11 @@ struct Bufs {
     HomeCell *home = nullptr;
     int32_t *counts = nullptr;
     int64_t *offsets = nullptr;
-    int *small = nullptr;  // [0] occupied cells, [1] error bits
+    int *small = nullptr;  // [0] occupied cells, [1] error bits, [2] matrix
+                           // overflow, [4..5] mask-pool cursor (u64)
+    uint32_t *mask_pool = nullptr;
+    long long mask_cap = 0;
+    long long *home_mask = nullptr;
 };
 
 struct Workspace {
@@ -73,6 +77,7 @@ struct Plan {
     int64_t batch_natoms = 0;
     int batch_nsys = 0;
     bool batch_fp32 = true;
+    int batch_kind = kCutScalar;
     int batch_grid = kGridDense;
     bool have_count = false;
     int64_t npairs = 0;
