@@ -132,6 +132,103 @@ class ClockSampler:
                 "samples": len(self.samples), "source": "nvml, 20 ms"}
 
 
+def batched_bench(steps, warmup, dev, rank=0):
+    """C4: 4,096 small systems (sizes log-uniform 8-512, random triclinic cells
+    scaled towards 0.08 A^-3, random pbc, per-atom radii 3-6 A, ijdDS).
+    Batched: the FP32-filter build of all systems replayed from one captured
+    CUDA graph.  Plain: one FP64 nbl_count + nbl_fill per system."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    from matscipy_neighbours import _workloads as W
+    from matscipy_neighbours.batch import NeighbourListBatch
+
+    systems = W.batched_systems(seed=1 + rank)
+    b = NeighbourListBatch(systems, precision="fp32", graph=True, autotune=True,
+                           device=dev.index)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        b.run()
+    npairs = b.npairs
+    ms = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        b.stream.wait_stream(stream)
+        e0.record(b.stream)
+        b.launch()
+        e1.record(b.stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    b.finish()
+    cfg = b.config()
+    positions = b.positions
+    offs = b.atom_offsets
+    b.close()
+
+    # plain per-system FP64 launches over the same resident positions
+    plan = ext.plan_for(dev.index)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    cap = int(npairs * 1.1) + 1024
+    outs = {"i": torch.empty(cap, dtype=torch.int32, device=dev),
+            "j": torch.empty(cap, dtype=torch.int32, device=dev),
+            "D": torch.empty((cap, 3), dtype=torch.float64, device=dev),
+            "d": torch.empty(cap, dtype=torch.float64, device=dev),
+            "S": torch.empty((cap, 3), dtype=torch.int32, device=dev)}
+    prev = ext.set_options(precision="fp64", grid="auto")
+    reqs = []
+    keep = []
+    for k, sd in enumerate(systems):
+        cell = np.ascontiguousarray(sd["cell"])
+        inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+        pbc8 = np.ascontiguousarray(np.asarray(sd["pbc"], dtype=np.uint8))
+        rc, pa, pt, nc = ext.resolve_cutoff(np.asarray(sd["cutoff"]), len(sd["positions"]))
+        origin = np.zeros(3)
+        keep.extend([cell, inv, pbc8, pa, origin])
+        pos_ptr = positions.data_ptr() + int(offs[k]) * 24
+        reqs.append(ext.make_request(31, origin, cell, inv, pbc8, len(sd["positions"]),
+                                     ctypes.c_void_p(pos_ptr), True, rc, pa, None, 0,
+                                     None, dev.index))
+    ext.set_options(**prev)
+
+    def plain_pass():
+        n = ctypes.c_int64()
+        base = 0
+        for r in reqs:
+            ext.check(ext.lib.nbl_count(plan, ctypes.byref(r), sptr, ctypes.byref(n)))
+            o = ext.Outputs()
+            o.first = outs["i"].data_ptr() + 4 * base
+            o.second = outs["j"].data_ptr() + 4 * base
+            o.distvec = outs["D"].data_ptr() + 24 * base
+            o.absdist = outs["d"].data_ptr() + 8 * base
+            o.shift = outs["S"].data_ptr() + 12 * base
+            ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sptr))
+            base += n.value
+        return base
+
+    plain_pass()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    tot = plain_pass()
+    torch.cuda.synchronize(dev)
+    plain_s = time.perf_counter() - t0
+    assert tot == npairs, (tot, npairs)
+    batched_s = statistics.median(ms) * 1e-3
+    return {"workload": "batched_4096_systems", "systems": len(systems),
+            "atoms": int(offs[-1]), "npairs": int(npairs),
+            "batched_fp32_graph": {"value": npairs / batched_s, "unit": UNIT,
+                                   "ms_per_step": batched_s * 1e3,
+                                   "launch_config": {"count_ctas_per_sm": cfg[0],
+                                                     "count_atoms_per_pass": cfg[1],
+                                                     "fill_ctas_per_sm": cfg[2]}},
+            "plain_fp64_per_system": {"value": npairs / plain_s, "unit": UNIT,
+                                      "ms_per_step": plain_s * 1e3},
+            "speedup": plain_s / batched_s}
+
+
 def cpu_baseline(steps=2):
     """The reference's CPU core on the same workload (rank 0, N = 1)."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -209,6 +306,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--reps", type=int, default=64,
                     help="FCC unit cells per edge (64 = the benchmark size; smaller "
                          "values make the small cases used for profiling)")
@@ -389,6 +487,8 @@ def main():
         "stage_ms": {"count_phase": statistics.mean(a - b for a, b in zip(step_ms, fill_ms)),
                      "fill": statistics.mean(fill_ms)},
     }
+    if not args.no_batched:
+        out["batched"] = batched_bench(min(args.steps, 20), args.warmup, dev, rank)
     if world == 1 and not args.no_cpu_baseline and args.reps == 64:
         out["cpu_baseline"] = cpu_baseline()
     print(json.dumps(out), flush=True)

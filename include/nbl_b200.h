@@ -187,6 +187,72 @@ NBL_API nbl_status nbl_neighbour_list_device(const nbl_request *req, void *strea
                                      nbl_device_result *result);
 NBL_API nbl_status nbl_device_result_free(nbl_device_result *result, void *stream);
 
+/* ---- batches: many independent systems, one launch sequence --------------
+   (Build-only form with no reference counterpart: the reference handles one
+   system per call, neighbour_list_gpu.hh:95-96.)  Each system has its own
+   cell, pbc and cutoff; atoms are concatenated system after system.  Outputs
+   are concatenated too: the pairs of system s are [sys_offsets[s],
+   sys_offsets[s+1]) and their i, j are indices within system s. */
+typedef struct nbl_system {
+    const double *cell_origin;  /* [3] host */
+    const double *cell;         /* [9] host, rows = lattice vectors */
+    const double *inv_cell;     /* [9] host */
+    const uint8_t *pbc;         /* [3] host */
+    int64_t nat;
+    double cutoff;              /* binning / global cutoff (per-atom: max 2r) */
+} nbl_system;
+
+typedef struct nbl_batch_request {
+    int quantities;
+    int32_t nsys;
+    const nbl_system *systems;          /* host [nsys] */
+    const double *positions;            /* [3*N] concatenated */
+    int positions_on_device;            /* 0: copied once into the batch */
+    const double *per_atom_cutoff;      /* [N] concatenated, or NULL */
+    const int32_t *types;               /* [N] or NULL */
+    const double *per_type_cutoff_sq;   /* [ncutoffs^2] host, shared, or NULL */
+    int32_t ncutoffs;
+    int aux_on_device;
+    int grid;                           /* nbl_grid */
+    int precision;                      /* nbl_precision */
+    int autotune;                       /* 1: time launch configurations at set-up */
+} nbl_batch_request;
+
+typedef struct nbl_batch_outputs {
+    int32_t *first;
+    int32_t *second;
+    double *distvec;
+    double *absdist;
+    int32_t *shift;
+    int64_t *sys_offsets;               /* [nsys+1] pair offset of each system */
+    int64_t capacity;                   /* pairs the output buffers hold */
+    double *positions;                  /* device positions the batch reads */
+} nbl_batch_outputs;
+
+typedef struct nbl_batch nbl_batch;
+
+NBL_API nbl_status nbl_batch_create(int device_id, nbl_batch **batch);
+NBL_API nbl_status nbl_batch_destroy(nbl_batch *batch);
+/* Plans every system, uploads the tables once and allocates device outputs for
+   `capacity` pairs (<= 0: the exact count plus 25 % headroom).  Synchronous. */
+NBL_API nbl_status nbl_batch_setup(nbl_batch *batch, const nbl_batch_request *req,
+                                   int64_t capacity);
+/* Enqueues the whole build on `stream` (NULL: the batch's own stream): no host
+   synchronisation and no allocation, so it can be captured in a CUDA graph. */
+NBL_API nbl_status nbl_batch_run(nbl_batch *batch, void *stream);
+/* Captures nbl_batch_run into a CUDA graph (stream must not be the legacy
+   default stream; NULL uses the batch's own stream). */
+NBL_API nbl_status nbl_batch_capture(nbl_batch *batch, void *stream);
+/* Replays the captured graph: one launch for the whole batch. */
+NBL_API nbl_status nbl_batch_launch(nbl_batch *batch, void *stream);
+/* Synchronises `stream`, returns the total pair count; NBL_ERROR_CAPACITY when
+   it exceeds the capacity (outputs then hold only the pairs that fit). */
+NBL_API nbl_status nbl_batch_finish(nbl_batch *batch, void *stream, int64_t *npairs);
+NBL_API nbl_status nbl_batch_get_outputs(nbl_batch *batch, nbl_batch_outputs *out);
+/* The launch configuration in use (chosen by the autotuner when enabled). */
+NBL_API nbl_status nbl_batch_get_config(nbl_batch *batch, int *count_mult,
+                                        int *count_group, int *fill_mult);
+
 /* Allocation-free variant of nbl_count + nbl_fill, for callers that cannot
    allocate device memory at call time (an MD loop that forbids allocation
    after start-up, a host whose pool allocator has reserved the device

@@ -224,6 +224,7 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     const int64_t mask_cap = std::max<int64_t>(int64_t(1) << 20, 16 * N);
     size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
     size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1));
+    size_t o_items = L.add(sizeof(int2) * std::max<int64_t>(N, 1));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
     if (st != NBL_SUCCESS) return st;
     char *base = static_cast<char *>(p.ws.base);
@@ -260,6 +261,7 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     B.mask_pool = (uint32_t *)at(o_mask);
     B.mask_cap = mask_cap;
     B.home_mask = (long long *)at(o_hmask);
+    B.items = (int2 *)at(o_items);
     return NBL_SUCCESS;
 }
 
@@ -321,14 +323,15 @@ nbl_status finish_batch(Batch &b, int grid_req) {
 // count / fill
 // ---------------------------------------------------------------------------
 
-static int traverse_grid(const Plan &p, int64_t natoms) {
-    // Persistent-style grid: a few resident CTAs per SM, capped by the number
-    // of possible home cells.
-    const int64_t g = std::min<int64_t>((int64_t)p.num_sms * 8, std::max<int64_t>(natoms, 1));
-    return (int)g;
+static int traverse_grid(const Plan &p, int64_t natoms, int mult) {
+    // Persistent-style grid: a few resident CTAs per SM (four warps each, one
+    // work item per warp at a time), capped by the number of work items.
+    const int64_t items = std::max<int64_t>((natoms + 3) / 4, 1);
+    return (int)std::min<int64_t>((int64_t)p.num_sms * mult, items);
 }
 
-nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
+// Size the workspace for a batch and copy its inputs and host tables in.
+nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
     nbl_status s = layout_workspace(p, b);
     if (s != NBL_SUCCESS) return s;
     Bufs &B = p.bufs;
@@ -391,7 +394,16 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
         NBL_CUDA(cudaEventRecord(p.stage_done, st), "staging event");
         p.stage_in_flight = true;
     }
+    return NBL_SUCCESS;
+}
 
+// Enqueue the count phase (bin, sort, gather, work items, count, scan) on a
+// batch whose inputs are resident: no host synchronisation, no allocation,
+// so it can be captured in a CUDA graph.
+nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
+    Bufs &B = p.bufs;
+    const int64_t N = b.natoms;
+    const int nsys = (int)b.sys.size();
     NBL_CUDA(cudaMemsetAsync(B.small, 0, sizeof(int) * 8, st), "memset");
     NBL_CUDA(cudaMemsetAsync(B.table, 0, sizeof(int2) * b.table_size, st), "memset table");
     if (b.grid == kGridHashed)
@@ -442,12 +454,16 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     ga.home = B.home;
     ga.n_home = n_home;
     NBL_CUDA(launch_gather(ga, st), "k_gather");
+    NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms, st),
+             "k_tiles");
 
     TraverseArgs &ta = p.targs;
     std::memset(&ta, 0, sizeof(ta));
     ta.sys = B.sys;
     ta.home = B.home;
     ta.n_home = n_home;
+    ta.items = B.items;
+    ta.n_items = B.small + 3;
     ta.grid = b.grid;
     ta.table = B.table;
     ta.hkey = B.hkey;
@@ -465,12 +481,23 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     ta.mask_cap = B.mask_cap;
     ta.home_mask = B.home_mask;
     ta.err = err;
-    p.trav_grid = traverse_grid(p, N);
+    p.trav_grid = traverse_grid(p, N, p.count_mult);
+    p.fill_grid = traverse_grid(p, N, p.fill_mult);
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
-    NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st),
+    NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
+                             p.count_group),
              "count pass");
     NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
+    return NBL_SUCCESS;
+}
 
+nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
+    nbl_status s = upload_batch(p, b, st);
+    if (s != NBL_SUCCESS) return s;
+    s = enqueue_count(p, b, st);
+    if (s != NBL_SUCCESS) return s;
+    Bufs &B = p.bufs;
+    const int64_t N = b.natoms;
     if (sync) {
         NBL_CUDA(cudaMemcpyAsync(p.host_small, B.offsets + N, sizeof(int64_t),
                                  cudaMemcpyDeviceToHost, st), "read pair count");
@@ -502,7 +529,7 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     ta.shift = o.shift;
     ta.capacity = capacity;
     if (!(o.first || o.second || o.distvec || o.absdist || o.shift)) return NBL_SUCCESS;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.trav_grid, st),
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st),
              "fill pass");
     return NBL_SUCCESS;
 }
@@ -764,7 +791,7 @@ nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
     ta.mat_count = count;
     ta.mat_overflow = p.bufs.small + 2;
     ta.capacity = 0;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.trav_grid, st),
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st),
              "matrix fill");
     NBL_CUDA(cudaMemcpyAsync(p.host_small + 2, p.bufs.small + 2, sizeof(int),
                              cudaMemcpyDeviceToHost, st), "read overflow");

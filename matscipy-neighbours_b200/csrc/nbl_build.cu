@@ -25,6 +25,7 @@
 // count, and in the fill pass the hits go into a per-warp queue that is
 // drained 32 pairs at a time so that the FP64 epilogue and the stores run
 // with full warps and near-contiguous addresses.
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <type_traits>
@@ -228,6 +229,46 @@ k_gather(GatherArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// k_tiles: work items = (occupied cell, 32-atom i-tile)
+// ---------------------------------------------------------------------------
+// Splitting large cells keeps one warp from holding a whole big cell (a
+// small periodic system often is one cell) while the rest of the GPU idles.
+__global__ void __launch_bounds__(256)
+k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
+        const int2 *__restrict__ table, int2 *__restrict__ items, int *__restrict__ n_items) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int nh = *n_home;
+    for (int base = blockIdx.x * blockDim.x; base < nh; base += gridDim.x * blockDim.x) {
+        const int h = base + threadIdx.x;
+        int2 hs = make_int2(0, 0);
+        if (h < nh) hs = table[home[h].tidx];
+        const int nt = (hs.y - hs.x + 31) >> 5;
+        int incl = nt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(full, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const int tot = __shfl_sync(full, incl, 31);
+        int first = 0;
+        if (lane == 0 && tot > 0) first = atomicAdd(n_items, tot);
+        first = __shfl_sync(full, first, 0) + incl - nt;
+        for (int t = 0; t < nt; t++) items[first + t] = make_int2(h, hs.x + 32 * t);
+    }
+}
+
+cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
+                         int2 *items, int *n_items, int64_t natoms, int num_sms,
+                         cudaStream_t st) {
+    if (natoms <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>((natoms + 255) / 256, (int64_t)num_sms * 4);
+    k_tiles<<<(unsigned)blocks, 256, 0, st>>>(home, n_home, table, items, n_items);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // The pair passes: k_count and k_fill
 // ---------------------------------------------------------------------------
 //
@@ -256,7 +297,6 @@ constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSeg = 32;         // visited offsets per batch (one per lane)
 constexpr int kITile = 32;       // atoms i per i-tile
-constexpr int kGroup = 4;        // atoms swept together in the FP32 count
 constexpr int kWinWords = 256;   // hit words per emission window
 constexpr int kRange = kWinWords * 32;  // candidates per emission range
 constexpr float kFarCand = 1.0e18f;     // padding candidate
@@ -588,7 +628,7 @@ __device__ __forceinline__ int div_small(int w, int n, float inv_n) {
 
 }  // namespace
 
-template <bool FP32, int KIND>
+template <bool FP32, int KIND, int GROUP>
 __global__ void __launch_bounds__(kThreads, 6)
 k_count(TraverseArgs a) {
     constexpr int kCand = CountTile<FP32>::kCand;
@@ -596,17 +636,19 @@ k_count(TraverseArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CountSmem<FP32> &sm = smem[warp];
     const unsigned full = 0xffffffffu;
-    const int nhome = *a.n_home;
+    const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    for (int h = gwarp; h < nhome; h += nwarps) {
-        const Home c = load_home<FP32>(a, h);
+    for (int it = gwarp; it < nitems; it += nwarps) {
+        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
+        const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
         const int2 hs = c.hs;
         const bool one_batch = c.nvisit <= kSeg;
         long long mbase = -1;
 
-        for (int ib = hs.x; ib < hs.y; ib += kITile) {
+        {
+            const int ib = item.y;
             const int ni = min(kITile, hs.y - ib);
             if (lane < ni) {
                 sm.i32[lane] = a.pos32[ib + lane];
@@ -617,18 +659,18 @@ k_count(TraverseArgs a) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 const int nchunks_all = (total + 31) >> 5;
-                // One word region per home cell, taken with its first i-tile:
-                // (atoms of the cell) x (chunks of the candidate list).
-                if (ib == hs.x && vb == 0 && a.mask_pool != nullptr) {
+                // One word region per work item: (atoms of the i-tile) x (chunks
+                // of the candidate list).
+                if (vb == 0 && a.mask_pool != nullptr) {
                     long long base = -1;
                     if (lane == 0 && one_batch && nchunks_all <= kWinWords) {
-                        const long long words = (long long)(hs.y - hs.x) * nchunks_all;
+                        const long long words = (long long)ni * nchunks_all;
                         const unsigned long long b =
                             atomicAdd(a.mask_cursor, (unsigned long long)words);
                         if ((long long)b + words <= a.mask_cap) base = (long long)b;
                     }
                     base = __shfl_sync(full, base, 0);
-                    if (lane == 0) a.home_mask[h] = base;
+                    if (lane == 0) a.home_mask[it] = base;
                     mbase = base;
                 }
                 // candidate index of atom si itself at offset 0 is kself0 + si
@@ -640,13 +682,13 @@ k_count(TraverseArgs a) {
                     const int nck = nkp >> 5;
                     stage<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
                     if constexpr (FP32) {
-                        // kGroup atoms per pass over the tile
-                        for (int g0 = 0; g0 < ni; g0 += kGroup) {
-                            float4 pg[kGroup];
-                            int ks[kGroup], cnt[kGroup];
-                            unsigned mw[kGroup];
+                        // GROUP atoms per pass over the tile
+                        for (int g0 = 0; g0 < ni; g0 += GROUP) {
+                            float4 pg[GROUP];
+                            int ks[GROUP], cnt[GROUP];
+                            unsigned mw[GROUP];
 #pragma unroll
-                            for (int g = 0; g < kGroup; g++) {
+                            for (int g = 0; g < GROUP; g++) {
                                 const bool v = g0 + g < ni;
                                 pg[g] = v ? sm.i32[g0 + g]
                                           : make_float4(kFarAtom, kFarAtom, kFarAtom, 0.f);
@@ -657,10 +699,10 @@ k_count(TraverseArgs a) {
                             for (int ch = 0; ch < nck; ch++) {
                                 const int k = ch * 32 + lane;
                                 const float4 cv = sm.cand[k];
-                                unsigned m[kGroup];
-                                bool amb_any = false, amb[kGroup];
+                                unsigned m[GROUP];
+                                bool amb_any = false, amb[GROUP];
 #pragma unroll
-                                for (int g = 0; g < kGroup; g++) {
+                                for (int g = 0; g < GROUP; g++) {
                                     const float dx = cv.x - pg[g].x;
                                     const float dy = cv.y - pg[g].y;
                                     const float dz = cv.z - pg[g].z;
@@ -674,7 +716,7 @@ k_count(TraverseArgs a) {
                                 }
                                 if (__any_sync(full, amb_any)) {
 #pragma unroll
-                                    for (int g = 0; g < kGroup; g++) {
+                                    for (int g = 0; g < GROUP; g++) {
                                         bool h2 = false;
                                         if (amb[g])
                                             h2 = resolve_exact<KIND>(sm.sg, a, H, nseg, kb + k,
@@ -684,24 +726,24 @@ k_count(TraverseArgs a) {
                                 }
                                 const bool mine = lane == (ch & 31);
 #pragma unroll
-                                for (int g = 0; g < kGroup; g++) {
+                                for (int g = 0; g < GROUP; g++) {
                                     cnt[g] += __popc(m[g]);
                                     mw[g] = mine ? m[g] : mw[g];
                                 }
                                 if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
                                     const long long w0 = mbase + (kb >> 5) + (ch & ~31) + lane;
 #pragma unroll
-                                    for (int g = 0; g < kGroup; g++) {
+                                    for (int g = 0; g < GROUP; g++) {
                                         if (g0 + g < ni && lane <= (ch & 31))
-                                            a.mask_pool[w0 + (long long)(ib + g0 + g - hs.x) *
+                                            a.mask_pool[w0 + (long long)(g0 + g) *
                                                                  nchunks_all] = mw[g];
                                     }
                                 }
                             }
-                            if (lane < kGroup && g0 + lane < ni) {
+                            if (lane < GROUP && g0 + lane < ni) {
                                 int cg = cnt[0];
 #pragma unroll
-                                for (int g = 1; g < kGroup; g++)
+                                for (int g = 1; g < GROUP; g++)
                                     if (lane == g) cg = cnt[g];
                                 sm.icount[g0 + lane] += cg;
                             }
@@ -723,7 +765,7 @@ k_count(TraverseArgs a) {
                                 mword = (lane == (ch & 31)) ? mask : mword;
                                 if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
                                     if (lane <= (ch & 31))
-                                        a.mask_pool[mbase + (long long)(si - hs.x) * nchunks_all +
+                                        a.mask_pool[mbase + (long long)(si - ib) * nchunks_all +
                                                     (kb >> 5) + (ch & ~31) + lane] = mword;
                                 }
                             }
@@ -828,15 +870,15 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
     }
     if (a.distvec) {
         double *D = a.distvec + 3 * slot;
-        D[0] = dx;
-        D[1] = dy;
-        D[2] = dz;
+        __stcs(D, dx);
+        __stcs(D + 1, dy);
+        __stcs(D + 2, dz);
     }
     if (a.shift) {
         int32_t *Sv = a.shift + 3 * slot;
-        Sv[0] = ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0];
-        Sv[1] = ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1];
-        Sv[2] = ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + sm.sg.m[seg][2];
+        __stcs(Sv, ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0]);
+        __stcs(Sv + 1, ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1]);
+        __stcs(Sv + 2, ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + sm.sg.m[seg][2]);
     }
 }
 
@@ -848,18 +890,20 @@ k_fill(TraverseArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FillSmem<FP32> &sm = smem[warp];
     const unsigned full = 0xffffffffu;
-    const int nhome = *a.n_home;
+    const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    for (int h = gwarp; h < nhome; h += nwarps) {
-        const Home c = load_home<FP32>(a, h);
+    for (int it = gwarp; it < nitems; it += nwarps) {
+        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
+        const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
         const int2 hs = c.hs;
         const bool one_batch = c.nvisit <= kSeg;
         const long long mbase =
-            (a.mask_pool != nullptr && one_batch) ? a.home_mask[h] : -1ll;
+            (a.mask_pool != nullptr && one_batch) ? a.home_mask[it] : -1ll;
 
-        for (int ib = hs.x; ib < hs.y; ib += kITile) {
+        {
+            const int ib = item.y;
             const int ni = min(kITile, hs.y - ib);
             if (lane < ni) {
                 const int si = ib + lane;
@@ -890,9 +934,8 @@ k_fill(TraverseArgs a) {
                         if (mbase >= 0) {
                             for (int w = lane; w < nw; w += 32) {
                                 const int al = div_small(w, nch, inv_nch);
-                                sm.mw[w] = a.mask_pool[mbase +
-                                                       (long long)(ib + a0 + al - hs.x) *
-                                                           nchunks + (kr >> 5) + (w - al * nch)];
+                                sm.mw[w] = a.mask_pool[mbase + (long long)(a0 + al) * nchunks +
+                                                       (kr >> 5) + (w - al * nch)];
                             }
                         } else {
                             for (int kt = 0; kt < nrange; kt += kCand) {
@@ -965,7 +1008,8 @@ k_fill(TraverseArgs a) {
 }
 
 #define NBL_INST(F, K)                                            \
-    template __global__ void k_count<F, K>(TraverseArgs);         \
+    template __global__ void k_count<F, K, 2>(TraverseArgs);      \
+    template __global__ void k_count<F, K, 4>(TraverseArgs);      \
     template __global__ void k_fill<F, K>(TraverseArgs);
 NBL_INST(true, kCutScalar)
 NBL_INST(true, kCutPerAtom)
@@ -992,31 +1036,39 @@ cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st) {
 }
 
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
-                            int grid, cudaStream_t st) {
+                            int grid, cudaStream_t st, int group) {
     if (grid <= 0) return cudaSuccess;
-#define NBL_GO(KERNEL, F, K) KERNEL<F, K><<<grid, kThreads, 0, st>>>(a)
-#define NBL_BY_KIND(KERNEL, F)                        \
+#define NBL_GO_C(F, K)                                                     \
+    do {                                                                   \
+        if (group == 2)                                                    \
+            k_count<F, K, 2><<<grid, kThreads, 0, st>>>(a);                \
+        else                                                               \
+            k_count<F, K, 4><<<grid, kThreads, 0, st>>>(a);                \
+    } while (0)
+#define NBL_GO_F(F, K) k_fill<F, K><<<grid, kThreads, 0, st>>>(a)
+#define NBL_BY_KIND(GO, F)                            \
     do {                                              \
         if (kind == kCutPerAtom)                      \
-            NBL_GO(KERNEL, F, kCutPerAtom);           \
+            GO(F, kCutPerAtom);                       \
         else if (kind == kCutPerType)                 \
-            NBL_GO(KERNEL, F, kCutPerType);           \
+            GO(F, kCutPerType);                       \
         else                                          \
-            NBL_GO(KERNEL, F, kCutScalar);            \
+            GO(F, kCutScalar);                        \
     } while (0)
     if (mode == kModeCount) {
         if (fp32)
-            NBL_BY_KIND(k_count, true);
+            NBL_BY_KIND(NBL_GO_C, true);
         else
-            NBL_BY_KIND(k_count, false);
+            NBL_BY_KIND(NBL_GO_C, false);
     } else {
         if (fp32)
-            NBL_BY_KIND(k_fill, true);
+            NBL_BY_KIND(NBL_GO_F, true);
         else
-            NBL_BY_KIND(k_fill, false);
+            NBL_BY_KIND(NBL_GO_F, false);
     }
 #undef NBL_BY_KIND
-#undef NBL_GO
+#undef NBL_GO_C
+#undef NBL_GO_F
     count_launch();
     return cudaGetLastError();
 }

@@ -50,6 +50,8 @@ struct TraverseArgs {
     const SysDev *sys;
     const HomeCell *home;
     const int *n_home;
+    const int2 *items;        // work items: (home cell, first atom of the i-tile)
+    const int *n_items;
     int grid;
     const int2 *table;
     const unsigned long long *hkey;
@@ -78,7 +80,7 @@ struct TraverseArgs {
     uint32_t *mask_pool;
     unsigned long long *mask_cursor;
     long long mask_cap;
-    long long *home_mask;
+    long long *home_mask;     // per work item
     int32_t mat_k;
     int32_t *mat_idx;
     double *mat_dist;
@@ -89,7 +91,11 @@ struct TraverseArgs {
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
+cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
+                         int2 *items, int *n_items, int64_t natoms, int num_sms,
+                         cudaStream_t st);
+// group: atoms swept together per pass in the FP32 count (2 or 4).
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
-                            int grid, cudaStream_t st);
+                            int grid, cudaStream_t st, int group = 4);
 
 }  // namespace nbl

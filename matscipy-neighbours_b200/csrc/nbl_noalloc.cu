@@ -170,6 +170,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     int32_t *counts = c.take<int32_t>(N + 1);
     int64_t *offsets = c.take<int64_t>(N + 1);
     int *small = c.take<int>(8);
+    int2 *items = c.take<int2>(std::max<int64_t>(N, 1));
     if (!c.ok)
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "nbl_neighbour_list_noalloc: the request needs more than the "
@@ -249,11 +250,16 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ga.home = home;
     ga.n_home = small;
     NA_CUDA(launch_gather(ga, s), "k_gather");
+    int nsm_tiles = 148;
+    cudaDeviceGetAttribute(&nsm_tiles, cudaDevAttrMultiProcessorCount, dev);
+    NA_CUDA(launch_tiles(home, small, table, items, small + 3, N, nsm_tiles, s), "k_tiles");
 
     TraverseArgs ta{};
     ta.sys = sys;
     ta.home = home;
     ta.n_home = small;
+    ta.items = items;
+    ta.n_items = small + 3;
     ta.grid = b.grid;
     ta.table = table;
     ta.hkey = hkey;

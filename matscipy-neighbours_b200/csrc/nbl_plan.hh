@@ -53,10 +53,12 @@ struct Bufs {
     int32_t *counts = nullptr;
     int64_t *offsets = nullptr;
     int *small = nullptr;  // [0] occupied cells, [1] error bits, [2] matrix
-                           // overflow, [4..5] mask-pool cursor (u64)
+                           // overflow, [3] work items, [4..5] mask-pool cursor
+                           // (u64)
     uint32_t *mask_pool = nullptr;
     long long mask_cap = 0;
     long long *home_mask = nullptr;
+    int2 *items = nullptr;
 };
 
 struct Workspace {
@@ -73,7 +75,13 @@ struct Plan {
     Workspace ws;
     Bufs bufs;
     TraverseArgs targs{};
-    int trav_grid = 0;
+    int trav_grid = 0;        // count-pass grid (CTAs)
+    int fill_grid = 0;        // fill-pass grid (CTAs)
+    // Launch configuration (set by the autotuner for batches): CTAs per SM
+    // of the count and fill passes, atoms per sweep pass in the count.
+    int count_mult = 8;
+    int fill_mult = 8;
+    int count_group = 4;
     int64_t batch_natoms = 0;
     int batch_nsys = 0;
     bool batch_fp32 = true;
@@ -95,6 +103,8 @@ nbl_status plan_system(const double origin[3], const double cell[9],
                        const double inv_cell[9], const uint8_t pbc[3], double cutoff,
                        SysDev &S, int64_t &ncells);
 nbl_status finish_batch(Batch &b, int grid_req);
+nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st);
+nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st);
 nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync);
 nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_t st);
 nbl_status read_flags(Plan &p, cudaStream_t st);
