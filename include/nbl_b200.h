@@ -253,6 +253,33 @@ NBL_API nbl_status nbl_batch_get_outputs(nbl_batch *batch, nbl_batch_outputs *ou
 NBL_API nbl_status nbl_batch_get_config(nbl_batch *batch, int *count_mult,
                                         int *count_group, int *fill_mult);
 
+/* ---- backward: gradients through the pair list -------------------------
+   (Build-only form with no reference counterpart.)  For a fixed pair list of
+   one system, D = r_j - r_i + sum_m c_m cell[m] with c_m = S_m on periodic
+   axes and 0 on non-periodic ones, and d = |D|.  Given dL/dD and/or dL/dd,
+   writes dL/dpositions [nat*3] and dL/dcell [9] (row-major, cell rows =
+   lattice vectors).  All pointers are device pointers except pbc.  With
+   deterministic != 0 the result is bit-reproducible (the j-side is reduced
+   after a stable sort by j instead of with atomics). */
+typedef struct nbl_backward_args {
+    int64_t npairs;
+    int64_t nat;
+    const int32_t *first;          /* [npairs], sorted (as the fill writes it) */
+    const int32_t *second;         /* [npairs] */
+    const int32_t *shift;          /* [3*npairs] */
+    const double *distvec;         /* [3*npairs] (needed with grad_absdist) */
+    const double *absdist;         /* [npairs]   (needed with grad_absdist) */
+    const double *grad_distvec;    /* [3*npairs] or NULL */
+    const double *grad_absdist;    /* [npairs] or NULL */
+    const int64_t *row_offsets;    /* [nat+1] (nbl_row_offsets) or NULL */
+    const uint8_t *pbc;            /* [3] host */
+    double *grad_positions;        /* [3*nat] out */
+    double *grad_cell;             /* [9] out */
+    int deterministic;
+} nbl_backward_args;
+
+NBL_API nbl_status nbl_backward(const nbl_backward_args *args, void *stream);
+
 /* Allocation-free variant of nbl_count + nbl_fill, for callers that cannot
    allocate device memory at call time (an MD loop that forbids allocation
    after start-up, a host whose pool allocator has reserved the device
