@@ -131,6 +131,18 @@ NBL_API nbl_status nbl_plan_destroy(nbl_plan *plan);
 /* Releases the plan's device workspace (it is re-grown on the next call). */
 NBL_API nbl_status nbl_plan_trim(nbl_plan *plan);
 
+/* Row split: later nbl_count / nbl_fill calls on this plan produce only the
+   rows i with lo <= i < hi (original atom indices; every atom stays a
+   candidate j).  The pair count and the output are then exactly the slice
+   [offsets[lo], offsets[hi]) of the full list, so ranks that each take one
+   contiguous range reproduce the full list by concatenation.  hi < 0 means
+   "to the end"; lo = 0, hi = -1 restores the full list.  The range takes
+   effect at the next nbl_count, and a fill always uses its count's range, so
+   it may be reset between the two.  No reference
+   counterpart: the reference builds one list per process
+   (src/libneighbours/neighbour_list.cc:99-204). */
+NBL_API nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi);
+
 /* Count phase: bins the atoms, counts every atom's neighbours and scans the
    counts into row offsets.  Host positions are copied in on `stream`.
    Synchronises `stream` to return the pair count. */

@@ -481,6 +481,10 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.mask_cap = B.mask_cap;
     ta.home_mask = B.home_mask;
     ta.err = err;
+    ta.i_lo = p.i_lo;
+    ta.i_hi = p.i_hi;
+    if (p.i_lo > 0 || p.i_hi < N)
+        NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     p.trav_grid = traverse_grid(p, N, p.count_mult);
     p.fill_grid = traverse_grid(p, N, p.fill_mult);
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
@@ -689,6 +693,18 @@ nbl_status nbl_plan_trim(nbl_plan *plan) {
     cudaDeviceSynchronize();
     plan->p.ws.release();
     plan->p.have_count = false;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi) {
+    clear_error();
+    if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan");
+    if (hi < 0) hi = INT64_MAX;
+    if (lo < 0 || lo > hi)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "bad atom range [%lld, %lld)",
+                         (long long)lo, (long long)hi);
+    plan->p.i_lo = lo;
+    plan->p.i_hi = hi;
     return NBL_SUCCESS;
 }
 

@@ -327,6 +327,7 @@ struct __align__(16) CountSmem {
     CandT<FP32> cand[CountTile<FP32>::kCand];
     float4 i32[kITile];
     int32_t iatom[kITile];
+    int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     int32_t icount[kITile];
 };
 
@@ -339,6 +340,7 @@ struct __align__(16) FillSmem {
     double4 i64[kITile];
     float4 i32[kITile];
     int4 iaux[kITile];
+    int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     long long icur[kITile];
     uint32_t mw[kWinWords];
     int32_t mpre[kWinWords + 1];
@@ -649,12 +651,29 @@ k_count(TraverseArgs a) {
 
         {
             const int ib = item.y;
-            const int ni = min(kITile, hs.y - ib);
-            if (lane < ni) {
-                sm.i32[lane] = a.pos32[ib + lane];
-                sm.iatom[lane] = a.aux[ib + lane].x;
-                sm.icount[lane] = 0;
+            // The tile's atoms whose original index lies in [i_lo, i_hi),
+            // compacted in order (all of them unless the rows are split).
+            int ni;
+            {
+                const int nt = min(kITile, hs.y - ib);
+                int ax = 0;
+                bool in = false;
+                if (lane < nt) {
+                    ax = a.aux[ib + lane].x;
+                    in = ax >= a.i_lo && ax < a.i_hi;
+                }
+                const unsigned im = __ballot_sync(full, in);
+                ni = __popc(im);
+                if (in) {
+                    const int c2 = __popc(im & lanemask_lt());
+                    sm.i32[c2] = a.pos32[ib + lane];
+                    sm.iatom[c2] = ax;
+                    sm.isi[c2] = ib + lane;
+                    sm.icount[c2] = 0;
+                }
+                __syncwarp();
             }
+            if (ni == 0) continue;
             for (int vb = 0; vb < c.nvisit; vb += kSeg) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
@@ -692,7 +711,7 @@ k_count(TraverseArgs a) {
                                 const bool v = g0 + g < ni;
                                 pg[g] = v ? sm.i32[g0 + g]
                                           : make_float4(kFarAtom, kFarAtom, kFarAtom, 0.f);
-                                ks[g] = v ? kself0 + (ib + g0 + g) - kb : -1;
+                                ks[g] = v ? kself0 + sm.isi[g0 + g] - kb : -1;
                                 cnt[g] = 0;
                                 mw[g] = 0u;
                             }
@@ -720,7 +739,7 @@ k_count(TraverseArgs a) {
                                         bool h2 = false;
                                         if (amb[g])
                                             h2 = resolve_exact<KIND>(sm.sg, a, H, nseg, kb + k,
-                                                                     ib + g0 + g, pg[g].w);
+                                                                     sm.isi[g0 + g], pg[g].w);
                                         m[g] |= __ballot_sync(full, h2);
                                     }
                                 }
@@ -751,7 +770,7 @@ k_count(TraverseArgs a) {
                         }
                     } else {
                         for (int il = 0; il < ni; il++) {
-                            const int si = ib + il;
+                            const int si = sm.isi[il];
                             const float4 pi32 = sm.i32[il];
                             const double4 pi64 = a.pos64[si];
                             const int kself_tile = kself0 + si - kb;
@@ -765,7 +784,7 @@ k_count(TraverseArgs a) {
                                 mword = (lane == (ch & 31)) ? mask : mword;
                                 if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
                                     if (lane <= (ch & 31))
-                                        a.mask_pool[mbase + (long long)(si - ib) * nchunks_all +
+                                        a.mask_pool[mbase + (long long)il * nchunks_all +
                                                     (kb >> 5) + (ch & ~31) + lane] = mword;
                                 }
                             }
@@ -904,15 +923,29 @@ k_fill(TraverseArgs a) {
 
         {
             const int ib = item.y;
-            const int ni = min(kITile, hs.y - ib);
-            if (lane < ni) {
-                const int si = ib + lane;
-                sm.i32[lane] = a.pos32[si];
-                sm.i64[lane] = a.pos64[si];
-                const int4 ax = a.aux[si];
-                sm.iaux[lane] = ax;
-                sm.icur[lane] = (long long)a.offsets[ax.x];
+            int ni;
+            {
+                const int nt = min(kITile, hs.y - ib);
+                int4 ax = make_int4(0, 0, 0, 0);
+                bool in = false;
+                if (lane < nt) {
+                    ax = a.aux[ib + lane];
+                    in = ax.x >= a.i_lo && ax.x < a.i_hi;
+                }
+                const unsigned im = __ballot_sync(full, in);
+                ni = __popc(im);
+                if (in) {
+                    const int c2 = __popc(im & lanemask_lt());
+                    const int si = ib + lane;
+                    sm.i32[c2] = a.pos32[si];
+                    sm.i64[c2] = a.pos64[si];
+                    sm.iaux[c2] = ax;
+                    sm.isi[c2] = si;
+                    sm.icur[c2] = (long long)a.offsets[ax.x];
+                }
+                __syncwarp();
             }
+            if (ni == 0) continue;
             for (int vb = 0; vb < c.nvisit; vb += kSeg) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
@@ -943,7 +976,7 @@ k_fill(TraverseArgs a) {
                                 const int nkp = (nk + 31) & ~31;
                                 stage<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
                                 for (int al = 0; al < na; al++) {
-                                    const int il = a0 + al, si = ib + il;
+                                    const int il = a0 + al, si = sm.isi[il];
                                     const float4 pi32 = sm.i32[il];
                                     const double4 pi64 = sm.i64[il];
                                     const int kself_tile = kself0 + si - (kr + kt);

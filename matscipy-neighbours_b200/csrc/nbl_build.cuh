@@ -87,6 +87,10 @@ struct TraverseArgs {
     int32_t *mat_count;
     int *mat_overflow;
     int *err;
+    // Rows produced: only atoms whose global index lies in [i_lo, i_hi) act
+    // as i; every atom stays a candidate j.  Rows outside keep count 0.
+    long long i_lo;
+    long long i_hi;
 };
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);

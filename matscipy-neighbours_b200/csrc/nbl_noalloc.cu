@@ -273,6 +273,8 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.counts = counts;
     ta.offsets = offsets;
     ta.err = small + 1;
+    ta.i_lo = 0;
+    ta.i_hi = INT64_MAX;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)std::min<int64_t>((int64_t)nsm * 6, std::max<int64_t>(N, 1));

@@ -82,6 +82,9 @@ struct Plan {
     int count_mult = 8;
     int fill_mult = 8;
     int count_group = 4;
+    // Row range of nbl_set_atom_range (global atom indices, [lo, hi)).
+    int64_t i_lo = 0;
+    int64_t i_hi = INT64_MAX;
     int64_t batch_natoms = 0;
     int batch_nsys = 0;
     bool batch_fp32 = true;

@@ -80,6 +80,7 @@ def _load():
         "nbl_plan_create": ([ctypes.c_int, ctypes.POINTER(P)], ctypes.c_int),
         "nbl_plan_destroy": ([P], ctypes.c_int),
         "nbl_plan_trim": ([P], ctypes.c_int),
+        "nbl_set_atom_range": ([P, ctypes.c_int64, ctypes.c_int64], ctypes.c_int),
         "nbl_count": ([P, ctypes.POINTER(Request), P, ctypes.POINTER(ctypes.c_int64)],
                       ctypes.c_int),
         "nbl_fill": ([P, ctypes.POINTER(Outputs), P], ctypes.c_int),
@@ -382,10 +383,11 @@ def import_device_positions(py_in):
 
 
 def run_device(quantities, origin, cell, inv, pbc8, pos_t, host_pos, rc, per_atom,
-               per_type_sq, ncut, types, flags, device_id):
+               per_type_sq, ncut, types, flags, device_id, atom_range=None):
     """Device (or host-uploaded) positions in, torch CUDA tensors out on the
     device's current stream (neighbour_list_gpu_device,
-    neighbour_list_gpu.hh:95-96)."""
+    neighbour_list_gpu.hh:95-96).  atom_range=(lo, hi) keeps only the rows
+    lo <= i < hi: the slice of the full list that those rows occupy."""
     torch = _torch()
     dev = torch.device("cuda", device_id)
     stream = torch.cuda.current_stream(dev)
@@ -402,8 +404,16 @@ def run_device(quantities, origin, cell, inv, pbc8, pos_t, host_pos, rc, per_ato
                        per_type_sq, ncut, types, device_id)
     npairs = ctypes.c_int64()
     with torch.cuda.device(dev):
-        check(lib.nbl_count(plan, ctypes.byref(req), ctypes.c_void_p(stream.cuda_stream),
-                            ctypes.byref(npairs)))
+        if atom_range is not None:
+            check(lib.nbl_set_atom_range(plan, int(atom_range[0]), int(atom_range[1])))
+        try:
+            check(lib.nbl_count(plan, ctypes.byref(req),
+                                ctypes.c_void_p(stream.cuda_stream), ctypes.byref(npairs)))
+        finally:
+            if atom_range is not None:
+                # The range applies to the count just made (and its fill);
+                # later calls on this thread's plan build full lists again.
+                lib.nbl_set_atom_range(plan, 0, -1)
         n = int(npairs.value)
         tdt = {np.int32: torch.int32, np.float64: torch.float64}
         bufs = {}
