@@ -126,6 +126,7 @@ nbl_status plan_system(const double origin[3], const double cell[9],
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "cutoff spans more than 2^24 neighbour cells per cell");
     S.nvisit = (int32_t)nvisit;
+    S.visit_base = -1;
     S.cutoff = cutoff;
     S.cutoff_sq = cutoff * cutoff;
     double off_max = 0.0;
@@ -189,6 +190,15 @@ static nbl_status ensure(void *&ptr, size_t &have, size_t need, const char *what
     return NBL_SUCCESS;
 }
 
+// Visit tables for all systems when their entries are few (the usual case:
+// 27 per system); with more, the pair kernels compute offsets per item.
+constexpr int64_t kVisitCap = int64_t(1) << 20;
+static int64_t visit_entries(const Batch &b) {
+    int64_t n = 0;
+    for (const SysDev &S : b.sys) n += S.nvisit;
+    return n <= kVisitCap ? n : 0;
+}
+
 // Carve the per-call buffers out of the plan's workspace.
 static nbl_status layout_workspace(Plan &p, const Batch &b) {
     const int64_t N = b.natoms;
@@ -200,6 +210,8 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_pa = (b.per_atom && !b.aux_on_device) ? L.add(sizeof(double) * N) : 0;
     size_t o_ty = (b.types && !b.aux_on_device) ? L.add(sizeof(int32_t) * N) : 0;
     size_t o_sys = L.add(sizeof(SysDev) * nsys);
+    const int64_t nvis = visit_entries(b);
+    size_t o_vis = nvis ? L.add(sizeof(VisitDev) * nvis) : 0;
     size_t o_sab = L.add(sizeof(int64_t) * nsys);
     size_t o_pt64 = L.add(sizeof(double) * std::max<size_t>(b.pt64.size(), 1));
     size_t o_pt32 = L.add(sizeof(float) * std::max<size_t>(b.pt64.size(), 1));
@@ -237,6 +249,7 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
                                          : (int32_t *)at(o_ty))
                       : nullptr;
     B.sys = (SysDev *)at(o_sys);
+    B.visit = nvis ? (VisitDev *)at(o_vis) : nullptr;
     B.sys_atom_base = (int64_t *)at(o_sab);
     B.pt64 = (double *)at(o_pt64);
     B.pt32 = (float *)at(o_pt32);
@@ -372,6 +385,14 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
         }
         char *h = static_cast<char *>(p.host_stage);
         std::memcpy(h, b.sys.data(), sizeof(SysDev) * nsys);
+        if (B.visit != nullptr) {
+            SysDev *hs = reinterpret_cast<SysDev *>(h);
+            int64_t base = 0;
+            for (int s2 = 0; s2 < nsys; s2++) {
+                hs[s2].visit_base = base;
+                base += hs[s2].nvisit;
+            }
+        }
         NBL_CUDA(cudaMemcpyAsync(B.sys, h, sizeof(SysDev) * nsys, cudaMemcpyHostToDevice, st),
                  "copy systems");
         h += sizeof(SysDev) * nsys;
@@ -456,10 +477,12 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     NBL_CUDA(launch_gather(ga, st), "k_gather");
     NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms, st),
              "k_tiles");
+    NBL_CUDA(launch_visit(B.sys, nsys, B.visit, st), "k_visit");
 
     TraverseArgs &ta = p.targs;
     std::memset(&ta, 0, sizeof(ta));
     ta.sys = B.sys;
+    ta.visit = B.visit;
     ta.home = B.home;
     ta.n_home = n_home;
     ta.items = B.items;

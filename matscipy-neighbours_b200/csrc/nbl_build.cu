@@ -316,6 +316,7 @@ struct FillTile {
 
 struct SegSmem {
     double off[kSeg][3];
+    float off32[kSeg][3];
     int32_t m[kSeg][3];
     int32_t b[kSeg];
     int32_t pref[kSeg + 1];
@@ -331,7 +332,10 @@ struct __align__(16) CountSmem {
     int32_t icount[kITile];
 };
 
-constexpr int kChunkSeg = 256;   // chunk -> first segment table (fill)
+constexpr int kCandTab = 1024;   // candidates with a segment-table entry (fill)
+constexpr int kPosTab = 960;     // pairs per window with a position table (fill)
+static_assert(kRange <= 8192 && kITile <= 32,
+              "position-table entries hold the candidate in 13 bits, the atom in 5");
 
 template <bool FP32>
 struct __align__(16) FillSmem {
@@ -344,7 +348,8 @@ struct __align__(16) FillSmem {
     long long icur[kITile];
     uint32_t mw[kWinWords];
     int32_t mpre[kWinWords + 1];
-    uint8_t chunk_seg[kChunkSeg];   // segment of candidate 32*c of the batch
+    uint32_t ptab[kPosTab];    // window position -> candidate | atom << 13 (small windows)
+    uint8_t cand_seg[kCandTab];     // segment of each of the batch's first candidates
 };
 
 // Per-home-cell constants kept in registers.
@@ -401,6 +406,18 @@ __device__ __forceinline__ int2 cell_lookup(const TraverseArgs &a, const SysDev 
     return hash_find(a.hkey, a.hmask, a.table, key, a.err);
 }
 
+// Offset vector of cell offset d (neighbour_visit.hh:67,73,80):
+// off3 = z b3; off2 = off3 + y b2; off = off2 + x b1, in FP64 without FMA.
+__device__ __forceinline__ void visit_offset(const SysDev &S, const int d[3], double o[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double v = dmul((double)d[2], S.bin[2][k]);
+        v = dadd(v, dmul((double)d[1], S.bin[1][k]));
+        v = dadd(v, dmul((double)d[0], S.bin[0][k]));
+        o[k] = v;
+    }
+}
+
 // Segment batch vb of a home cell: one lane per visited offset
 // (neighbour_visit.hh:63-84).  Returns the batch size, its candidate total
 // and the index of the zero-offset segment (-1 if not in this batch).
@@ -416,9 +433,27 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
     bool zero = false;
     if (lane < nseg) {
         const int v = vb + lane;
-        const int xr = v % wx, rest = v / wx;
-        const int yr = rest % wy, zr = rest / wy;
-        const int off3[3] = {xr - nx, yr - ny, zr - nz};
+        int off3[3];
+        double offd[3];
+        float off32[3];
+        if (S.visit_base >= 0) {
+            const VisitDev &e = a.visit[S.visit_base + v];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                off3[k] = e.d[k];
+                offd[k] = e.off[k];
+                off32[k] = e.off32[k];
+            }
+        } else {
+            const int xr = v % wx, rest = v / wx;
+            const int yr = rest % wy, zr = rest / wy;
+            off3[0] = xr - nx;
+            off3[1] = yr - ny;
+            off3[2] = zr - nz;
+            visit_offset(S, off3, offd);
+#pragma unroll
+            for (int k = 0; k < 3; k++) off32[k] = __double2float_rn(offd[k]);
+        }
         int32_t cj[3], m[3];
         bool ok = true;
 #pragma unroll
@@ -426,8 +461,17 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
             int32_t x = c.hc.c[k] + off3[k];
             m[k] = 0;
             if (S.pbc[k]) {
-                m[k] = floor_div(x, S.n[k]);
-                x -= m[k] * S.n[k];
+                const int32_t n = S.n[k];
+                if (x < 0 && x >= -n) {
+                    m[k] = -1;
+                    x += n;
+                } else if (x >= n && x < 2 * n) {
+                    m[k] = 1;
+                    x -= n;
+                } else if (x < 0 || x >= n) {
+                    m[k] = floor_div(x, n);
+                    x -= m[k] * n;
+                }
             } else if (x < 0 || x >= S.n[k]) {
                 ok = false;
             }
@@ -437,13 +481,10 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         if (ok) sl = cell_lookup(a, S, c.hc.sys, cj[0], cj[1], cj[2]);
         len = sl.y - sl.x;
         sg.b[lane] = sl.x;
-        // neighbour_visit.hh:67,73,80: off3 = z b3; off2 = off3 + y b2; off = off2 + x b1
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            double o = dmul((double)off3[2], S.bin[2][k]);
-            o = dadd(o, dmul((double)off3[1], S.bin[1][k]));
-            o = dadd(o, dmul((double)off3[0], S.bin[0][k]));
-            sg.off[lane][k] = o;
+            sg.off[lane][k] = offd[k];
+            sg.off32[lane][k] = off32[k];
             sg.m[lane][k] = m[k];
         }
         zero = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
@@ -489,9 +530,9 @@ __device__ __forceinline__ void stage(CandT<FP32> *cand, const SegSmem &sg,
             if constexpr (FP32) {
                 const float4 p = a.pos32[sj];
                 float4 cv;
-                cv.x = p.x + __double2float_rn(sg.off[seg][0]);
-                cv.y = p.y + __double2float_rn(sg.off[seg][1]);
-                cv.z = p.z + __double2float_rn(sg.off[seg][2]);
+                cv.x = p.x + sg.off32[seg][0];
+                cv.y = p.y + sg.off32[seg][1];
+                cv.z = p.z + sg.off32[seg][2];
                 cv.w = p.w;
                 cand[k] = cv;
             } else {
@@ -800,15 +841,10 @@ k_count(TraverseArgs a) {
     }
 }
 
-// Segment of candidate kk, starting from the chunk's first segment.
+// Segment of candidate kk of the batch: from the table, else by search.
 template <bool FP32>
-__device__ __forceinline__ int seg_of_fast(const FillSmem<FP32> &sm, int nseg,
-                                           int nchunks, int kk) {
-    const int c = kk >> 5;
-    if (c >= kChunkSeg || c >= nchunks) return seg_of(sm.sg, nseg, kk);
-    int seg = sm.chunk_seg[c];
-    while (seg + 1 < nseg && sm.sg.pref[seg + 1] <= kk) seg++;
-    return seg;
+__device__ __forceinline__ int seg_of_tab(const FillSmem<FP32> &sm, int nseg, int kk) {
+    return kk < kCandTab ? (int)sm.cand_seg[kk] : seg_of(sm.sg, nseg, kk);
 }
 
 // One output pair in flight: where it goes and the j-side data it needs.
@@ -825,27 +861,34 @@ template <bool FP32>
 __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
                                                const TraverseArgs &a, int nseg, int nchunks,
                                                int nw, int nch, float inv_nch, int kr,
-                                               int a0, int total_w, int P) {
+                                               int a0, int total_w, int P, bool tab) {
     PairWork w;
     w.act = P < total_w;
     w.il = 0;
     w.seg = 0;
     w.slot = 0;
     if (w.act) {
-        int lo = 0, hi = nw - 1;  // last word with mpre <= P
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (sm.mpre[mid] <= P)
-                lo = mid;
-            else
-                hi = mid - 1;
+        int al, kk;
+        if (tab) {
+            const uint32_t e = sm.ptab[P];
+            al = (int)(e >> 13);
+            kk = kr + (int)(e & 8191u);
+        } else {
+            int lo = 0, hi = nw - 1;  // last word with mpre <= P
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sm.mpre[mid] <= P)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int bit = nth_set_bit(sm.mw[lo], P - sm.mpre[lo]);
+            al = div_small(lo, nch, inv_nch);
+            kk = kr + (lo - al * nch) * 32 + bit;
         }
-        const int bit = nth_set_bit(sm.mw[lo], P - sm.mpre[lo]);
-        const int al = div_small(lo, nch, inv_nch);
-        const int kk = kr + (lo - al * nch) * 32 + bit;
         w.il = a0 + al;
         w.slot = sm.icur[w.il] + (P - sm.mpre[al * nch]);
-        w.seg = seg_of_fast(sm, nseg, nchunks, kk);
+        w.seg = seg_of_tab(sm, nseg, kk);
         const int32_t sj = sm.sg.b[w.seg] + (kk - sm.sg.pref[w.seg]);
         w.pj = a.pos64[sj];
         w.aj = a.aux[sj];
@@ -950,8 +993,11 @@ k_fill(TraverseArgs a) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 const int nchunks = (total + 31) >> 5;
-                for (int cc = lane; cc < nchunks && cc < kChunkSeg; cc += 32)
-                    sm.chunk_seg[cc] = (uint8_t)seg_of(sm.sg, nseg, cc * 32);
+                // segment of each tabled candidate: lane = segment
+                if (lane < nseg) {
+                    const int e = min(sm.sg.pref[lane + 1], kCandTab);
+                    for (int k = sm.sg.pref[lane]; k < e; k++) sm.cand_seg[k] = (uint8_t)lane;
+                }
                 __syncwarp();
                 const int kself0 = (zs >= 0) ? sm.sg.pref[zs] - sm.sg.b[zs] : INT_MIN / 2;
 
@@ -1006,14 +1052,33 @@ k_fill(TraverseArgs a) {
                         }
                         if (lane == 0) sm.mpre[nw] = carry;
                         __syncwarp();
+                        // --- small windows: each word writes its bits' positions into
+                        //     a table (lane = word, ffs over its set bits), so a lane
+                        //     finds its pair with one shared-memory load --------------
+                        const bool tab = carry <= kPosTab;
+                        if (tab) {
+                            for (int w = lane; w < nw; w += 32) {
+                                unsigned word = sm.mw[w];
+                                int pos = sm.mpre[w];
+                                const int al = div_small(w, nch, inv_nch);
+                                const uint32_t base =
+                                    (uint32_t)((w - al * nch) * 32) | ((uint32_t)al << 13);
+                                while (word) {
+                                    const int b = __ffs(word) - 1;
+                                    word &= word - 1u;
+                                    sm.ptab[pos++] = base | (uint32_t)b;
+                                }
+                            }
+                            __syncwarp();
+                        }
                         // --- emission, software-pipelined: the next round's j-side
                         //     loads are in flight while the current round computes ----
                         PairWork cur = fetch_pair<FP32>(sm, a, nseg, nchunks, nw, nch,
-                                                        inv_nch, kr, a0, carry, lane);
+                                                        inv_nch, kr, a0, carry, lane, tab);
                         for (int P0 = 0; P0 < carry; P0 += 32) {
                             const PairWork nxt = fetch_pair<FP32>(sm, a, nseg, nchunks, nw,
                                                                   nch, inv_nch, kr, a0, carry,
-                                                                  P0 + 32 + lane);
+                                                                  P0 + 32 + lane, tab);
                             store_pair<FP32>(sm, a, H, cur);
                             cur = nxt;
                         }
@@ -1051,6 +1116,37 @@ NBL_INST(false, kCutScalar)
 NBL_INST(false, kCutPerAtom)
 NBL_INST(false, kCutPerType)
 #undef NBL_INST
+
+// One block per system with a visit table: its visited offsets in the
+// traversal's z/y/x order (neighbour_visit.hh:63-84).
+__global__ void k_visit(const SysDev *__restrict__ sys, VisitDev *__restrict__ visit) {
+    const SysDev &S = sys[blockIdx.x];
+    if (S.visit_base < 0) return;
+    const int nx = S.nscan[0], ny = S.nscan[1], nz = S.nscan[2];
+    const int wx = 2 * nx + 1, wy = 2 * ny + 1;
+    for (int v = threadIdx.x; v < S.nvisit; v += blockDim.x) {
+        const int xr = v % wx, rest = v / wx;
+        const int yr = rest % wy, zr = rest / wy;
+        const int d[3] = {xr - nx, yr - ny, zr - nz};
+        double o[3];
+        visit_offset(S, d, o);
+        VisitDev e;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            e.off[k] = o[k];
+            e.off32[k] = __double2float_rn(o[k]);
+            e.d[k] = d[k];
+        }
+        visit[S.visit_base + v] = e;
+    }
+}
+
+cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st) {
+    if (nsys <= 0 || visit == nullptr) return cudaSuccess;
+    k_visit<<<nsys, 64, 0, st>>>(sys, visit);
+    count_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st) {
     if (a.natoms <= 0) return cudaSuccess;

@@ -48,6 +48,7 @@ struct GatherArgs {
 
 struct TraverseArgs {
     const SysDev *sys;
+    const VisitDev *visit;    // per-system visit tables (systems with visit_base >= 0)
     const HomeCell *home;
     const int *n_home;
     const int2 *items;        // work items: (home cell, first atom of the i-tile)
@@ -95,6 +96,8 @@ struct TraverseArgs {
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
+// Fill the visit tables of the systems that have one (visit_base >= 0).
+cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
                          int2 *items, int *n_items, int64_t natoms, int num_sms,
                          cudaStream_t st);

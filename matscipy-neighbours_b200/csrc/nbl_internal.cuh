@@ -66,6 +66,16 @@ struct SysDev {
     int32_t ncutoffs;
     int32_t pt_base;     // first entry of this system's per-type tables
     int32_t nvisit;      // (2nx+1)(2ny+1)(2nz+1)
+    int64_t visit_base;  // first VisitDev entry of this system, -1: computed per item
+};
+
+// One visited neighbour offset of a system (neighbour_visit.hh:63-84): the
+// cell offset, the offset vector in FP64 (the reference's operation order)
+// and its FP32 rounding, computed once per call by k_visit.
+struct VisitDev {
+    double off[3];
+    float off32[3];
+    int32_t d[3];
 };
 
 struct HomeCell {

@@ -36,6 +36,7 @@ struct Bufs {
     double *per_atom = nullptr;
     int32_t *types = nullptr;
     SysDev *sys = nullptr;
+    VisitDev *visit = nullptr;     // per-system visit tables (nullptr: none)
     int64_t *sys_atom_base = nullptr;
     double *pt64 = nullptr;
     float *pt32 = nullptr;
