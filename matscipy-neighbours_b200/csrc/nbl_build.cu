@@ -272,25 +272,30 @@ cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *ta
 // The pair passes: k_count and k_fill
 // ---------------------------------------------------------------------------
 //
-// Both take one occupied home cell per WARP (warp-strided over the work list;
-// a CTA is four independent warps, so there is no block-wide barrier).  Per
-// home cell, one lane per visited neighbour offset computes the offset vector
-// (FP64, reference order), the wrap counts and the cell slice, and a warp scan
-// turns slice lengths into candidate positions (the "segment batch").
+// Both take one work item (home cell x i-tile of up to 32 atoms) per WARP
+// (warp-strided over the work list; a CTA is four independent warps, so there
+// is no block-wide barrier).  Per item, one lane per visited neighbour offset
+// reads the offset vector (FP64, reference order, from the per-system visit
+// table), the wrap counts and the cell slice, and a warp scan turns slice
+// lengths into candidate positions (the "segment batch").
 //
 // k_count stages the candidates in shared memory as FP32 positions in the
-// home-cell frame and sweeps them against the home cell's atoms, four atoms
-// per pass (independent FMA chains), 32 candidates per __ballot_sync.  Each
-// chunk's hit mask is popc'ed into the atom's count and, when the home cell
-// fits the mask pool, stored as one 32-bit word per (atom, chunk).
+// home-cell frame (lane = segment: each copies its cell's run of sorted
+// atoms) and sweeps them against the tile's atoms, GROUP atoms per pass
+// (independent FMA chains), 32 candidates per __ballot_sync.  Each chunk's
+// hit mask is popc'ed into the atom's count and, when the item fits the mask
+// pool, stored as one 32-bit word per (atom, chunk).
 //
 // k_fill turns hit words back into pairs lane-parallel: for a window of atoms
-// it builds the prefix of the words' popcounts, then lane L of each round takes
-// output position P = P0 + L, finds its word by binary search and its bit by an
-// n-th-set-bit search, and emits the pair at row_start + rank with exact FP64
-// D, d and S.  Consecutive lanes write consecutive slots.  Home cells without
-// pool words (pool full, more than one segment batch) recompute the words with
-// the same sweep first.
+// it builds the prefix of the words' popcounts; for windows of up to kPosTab
+// pairs each word then writes its set bits' (candidate, atom) codes at their
+// output positions (lane = word, ffs), so lane L of each round finds pair
+// P = P0 + L with one shared-memory load (larger windows search: binary
+// search over the prefix, then an n-th-set-bit search).  The pair (exact FP64
+// D, d and S) goes to row_start + rank, so consecutive lanes write
+// consecutive slots; the next round's j-side loads are issued before this
+// round's stores.  Items without pool words (pool full, more than one segment
+// batch) recompute the words with the count's sweep first.
 namespace {
 
 constexpr int kThreads = 128;
@@ -307,7 +312,7 @@ using CandT = typename std::conditional<FP32, float4, double4>::type;
 
 template <bool FP32>
 struct CountTile {
-    static constexpr int kCand = FP32 ? 256 : 128;
+    static constexpr int kCand = FP32 ? 384 : 192;
 };
 template <bool FP32>
 struct FillTile {
@@ -516,34 +521,33 @@ __device__ __forceinline__ int seg_of(const SegSmem &sg, int nseg, int kk) {
     return lo;
 }
 
-// Stage candidates kb .. kb+nk of the batch, padded to nkp with far points.
+// Stage candidates kb .. kb+nk of the batch segment by segment (lane =
+// segment: a run of consecutive sorted atoms), padded to nkp with far points.
 template <bool FP32>
-__device__ __forceinline__ void stage(CandT<FP32> *cand, const SegSmem &sg,
-                                      const TraverseArgs &a, int nseg, int kb, int nk,
-                                      int nkp, int lane) {
+__device__ __forceinline__ void stage_segs(CandT<FP32> *cand, const SegSmem &sg,
+                                           const TraverseArgs &a, int nseg, int kb, int nk,
+                                           int nkp, int lane) {
     __syncwarp();
-    for (int k = lane; k < nkp; k += 32) {
-        if (k < nk) {
-            const int kk = kb + k;
-            const int seg = seg_of(sg, nseg, kk);
-            const int sj = sg.b[seg] + (kk - sg.pref[seg]);
-            if constexpr (FP32) {
-                const float4 p = a.pos32[sj];
-                float4 cv;
-                cv.x = p.x + sg.off32[seg][0];
-                cv.y = p.y + sg.off32[seg][1];
-                cv.z = p.z + sg.off32[seg][2];
-                cv.w = p.w;
-                cand[k] = cv;
-            } else {
-                cand[k] = a.pos64[sj];
+    if (lane < nseg) {
+        const int s0 = max(sg.pref[lane], kb), s1 = min(sg.pref[lane + 1], kb + nk);
+        const int jb = sg.b[lane] - sg.pref[lane];
+        if constexpr (FP32) {
+            const float ox = sg.off32[lane][0], oy = sg.off32[lane][1], oz = sg.off32[lane][2];
+#pragma unroll 4
+            for (int kk = s0; kk < s1; kk++) {
+                const float4 p = a.pos32[jb + kk];
+                cand[kk - kb] = make_float4(p.x + ox, p.y + oy, p.z + oz, p.w);
             }
         } else {
-            if constexpr (FP32)
-                cand[k] = make_float4(kFarCand, kFarCand, kFarCand, 0.f);
-            else
-                cand[k] = make_double4(kFarCand, kFarCand, kFarCand, 0.0);
+#pragma unroll 4
+            for (int kk = s0; kk < s1; kk++) cand[kk - kb] = a.pos64[jb + kk];
         }
+    }
+    for (int k = nk + lane; k < nkp; k += 32) {
+        if constexpr (FP32)
+            cand[k] = make_float4(kFarCand, kFarCand, kFarCand, 0.f);
+        else
+            cand[k] = make_double4(kFarCand, kFarCand, kFarCand, 0.0);
     }
     __syncwarp();
 }
@@ -740,7 +744,7 @@ k_count(TraverseArgs a) {
                     const int nk = min(kCand, total - kb);
                     const int nkp = (nk + 31) & ~31;
                     const int nck = nkp >> 5;
-                    stage<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
+                    stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
                     if constexpr (FP32) {
                         // GROUP atoms per pass over the tile
                         for (int g0 = 0; g0 < ni; g0 += GROUP) {
@@ -1020,7 +1024,7 @@ k_fill(TraverseArgs a) {
                             for (int kt = 0; kt < nrange; kt += kCand) {
                                 const int nk = min(kCand, nrange - kt);
                                 const int nkp = (nk + 31) & ~31;
-                                stage<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
+                                stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
                                 for (int al = 0; al < na; al++) {
                                     const int il = a0 + al, si = sm.isi[il];
                                     const float4 pi32 = sm.i32[il];
