@@ -521,14 +521,30 @@ __device__ __forceinline__ int seg_of(const SegSmem &sg, int nseg, int kk) {
     return lo;
 }
 
-// Stage candidates kb .. kb+nk of the batch segment by segment (lane =
-// segment: a run of consecutive sorted atoms), padded to nkp with far points.
+// Stage candidates kb .. kb+nk of the batch, padded to nkp with far points.
+// Short cell runs (the usual case): lane = segment, each copying its cell's
+// run of consecutive sorted atoms.  Long runs: lane = candidate, the lane's
+// segment found once by search and then advanced as its candidate grows.
 template <bool FP32>
 __device__ __forceinline__ void stage_segs(CandT<FP32> *cand, const SegSmem &sg,
                                            const TraverseArgs &a, int nseg, int kb, int nk,
                                            int nkp, int lane) {
     __syncwarp();
-    if (lane < nseg) {
+    if (sg.pref[nseg] > 48 * nseg) {
+        int seg = lane < nk ? seg_of(sg, nseg, kb + lane) : 0;
+        for (int k = lane; k < nk; k += 32) {
+            const int kk = kb + k;
+            while (seg + 1 < nseg && sg.pref[seg + 1] <= kk) seg++;
+            const int sj = sg.b[seg] + (kk - sg.pref[seg]);
+            if constexpr (FP32) {
+                const float4 p = a.pos32[sj];
+                cand[k] = make_float4(p.x + sg.off32[seg][0], p.y + sg.off32[seg][1],
+                                      p.z + sg.off32[seg][2], p.w);
+            } else {
+                cand[k] = a.pos64[sj];
+            }
+        }
+    } else if (lane < nseg) {
         const int s0 = max(sg.pref[lane], kb), s1 = min(sg.pref[lane + 1], kb + nk);
         const int jb = sg.b[lane] - sg.pref[lane];
         if constexpr (FP32) {
