@@ -471,7 +471,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": _traffic_per_launch(npairs, nat),
-                     "kernel": "k_traverse<FILL> (fill pass)",
+                     "kernel": "k_fill (fill pass)",
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "fill_ms": statistics.mean(fill_ms)},
         "e2e": ({"value": e2e_value, "unit": UNIT,
