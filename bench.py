@@ -229,6 +229,133 @@ def batched_bench(steps, warmup, dev, rank=0):
             "speedup": plain_s / batched_s}
 
 
+def configs_bench(dev, flush, reps=10):
+    """The other configurations beside the headline (rank 0, N = 1): C1 plain
+    small, C3 sparse slab (per-type cutoffs, ijdD), C5 differentiation lattice.
+    Each: positions resident on the device, median of `reps` full builds
+    (count + fill) by CUDA events with the L2 flushed before each, and the
+    reference's CPU core on the same input (all host threads, median of 3).
+    C5 adds the backward kernel (nbl_backward, gradients of D and d), timed
+    alone, with its HBM roofline: npairs * 84 + nat * 48 algorithmic bytes."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    from matscipy_neighbours import _workloads as W
+    from matscipy_neighbours.autograd import BackwardArgs, _lib
+
+    peak, peak_kind, _ = _peaks()
+    cores = len(os.sched_getaffinity(0))
+    have_ref = O.ref_available()
+    if have_ref:
+        O.ref_set_threads(cores)
+    cpu_fn = O.ref_neighbour_list if have_ref else O.oracle_neighbour_list
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    plan = ext.plan_for(dev.index)
+    out = {}
+    for name, w in (("C1_plain_small", W.plain_small()),
+                    ("C3_sparse_slab", W.sparse_slab()),
+                    ("C5_diff_lattice", W.diff_lattice())):
+        q = w["quantities"]
+        flags = ext.quantity_flags(q)
+        nat = w["positions"].shape[0]
+        cell = np.ascontiguousarray(w["cell"], dtype=float)
+        inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+        pbc8 = np.ascontiguousarray(np.asarray(w["pbc"], dtype=np.uint8))
+        origin = np.zeros(3)
+        rc, pa, pt, nc = ext.resolve_cutoff(w["cutoff"], nat)
+        types = w.get("numbers")
+        types = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
+        pos = torch.from_numpy(np.ascontiguousarray(w["positions"])).to(dev)
+        req = ext.make_request(flags, origin, cell, inv, pbc8, nat,
+                               ctypes.c_void_p(pos.data_ptr()), True, rc, pa, pt, nc,
+                               types, dev.index)
+        n = ctypes.c_int64()
+        ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
+        npairs = int(n.value)
+        bufs = {"i": torch.empty(npairs, dtype=torch.int32, device=dev),
+                "j": torch.empty(npairs, dtype=torch.int32, device=dev),
+                "D": torch.empty((npairs, 3), dtype=torch.float64, device=dev),
+                "d": torch.empty(npairs, dtype=torch.float64, device=dev),
+                "S": torch.empty((npairs, 3), dtype=torch.int32, device=dev)}
+        o = ext._outputs_struct({c: bufs[c] for c in q}, lambda t: t.data_ptr())
+        ms = []
+        for k in range(reps + 3):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
+            ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sptr))
+            e1.record(stream)
+            e1.synchronize()
+            if k >= 3:
+                ms.append(e0.elapsed_time(e1))
+        ext.check(ext.lib.nbl_check(plan, sptr))
+        gpu_s = statistics.median(ms) * 1e-3
+        cpu_args = (q, w["cell"], w["positions"], w["cutoff"], w["pbc"])
+        cpu_fn(*cpu_args, types=types)
+        ct = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            cpu_fn(*cpu_args, types=types)
+            ct.append(time.perf_counter() - t0)
+        cpu_s = statistics.median(ct)
+        row = {"natoms": nat, "npairs": npairs, "quantities": q,
+               "gpu_ms": gpu_s * 1e3, "gpu_pairs_per_s": npairs / gpu_s,
+               "cpu_ms": cpu_s * 1e3, "cpu_pairs_per_s": npairs / cpu_s,
+               "cpu": {"kind": "reference" if have_ref else "port",
+                       "cores": cores if have_ref else 1},
+               "speedup": cpu_s / gpu_s}
+        if name.startswith("C5"):
+            off = torch.empty(nat + 1, dtype=torch.int64, device=dev)
+            ext.check(ext.lib.nbl_row_offsets(plan, ctypes.c_void_p(off.data_ptr()), sptr))
+            gen = torch.Generator(device=dev).manual_seed(0)
+            gD = torch.randn((npairs, 3), dtype=torch.float64, device=dev, generator=gen)
+            gd = torch.randn(npairs, dtype=torch.float64, device=dev, generator=gen)
+            gpos = torch.empty((nat, 3), dtype=torch.float64, device=dev)
+            gcell = torch.empty(9, dtype=torch.float64, device=dev)
+            a = BackwardArgs()
+            a.npairs, a.nat = npairs, nat
+            a.first, a.second = bufs["i"].data_ptr(), bufs["j"].data_ptr()
+            a.shift, a.distvec = bufs["S"].data_ptr(), bufs["D"].data_ptr()
+            a.absdist = bufs["d"].data_ptr()
+            a.grad_distvec, a.grad_absdist = gD.data_ptr(), gd.data_ptr()
+            a.row_offsets = off.data_ptr()
+            a.pbc = pbc8.ctypes.data
+            a.grad_positions, a.grad_cell = gpos.data_ptr(), gcell.data_ptr()
+            bl = _lib()
+            for det in (0, 1):
+                a.deterministic = det
+                # enqueued back to back (L2 flush between calls, outside the
+                # events), so the events time the device work, not the host
+                evs = []
+                for k in range(reps + 3):
+                    flush.zero_()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ext.check(bl.nbl_backward(ctypes.byref(a), sptr))
+                    e1.record(stream)
+                    evs.append((e0, e1))
+                torch.cuda.synchronize(dev)
+                bms = [e0.elapsed_time(e1) for e0, e1 in evs[3:]]
+                bt = statistics.median(bms) * 1e-3
+                alg = npairs * 84 + nat * 48
+                row["backward_deterministic" if det else "backward"] = {
+                    "ms": bt * 1e3, "achieved_gbs": alg / bt / 1e9,
+                    "frac": alg / bt / 1e9 / peak, "peak_gbs": peak,
+                    "peak_source": peak_kind, "algorithmic_bytes": alg}
+        out[name] = row
+    return out
+
+
 def cpu_baseline(steps=2):
     """The reference's CPU core on the same workload (rank 0, N = 1)."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -307,6 +434,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the C1/C3/C5 lines (and the backward timing)")
     ap.add_argument("--reps", type=int, default=64,
                     help="FCC unit cells per edge (64 = the benchmark size; smaller "
                          "values make the small cases used for profiling)")
@@ -489,6 +618,8 @@ def main():
     }
     if not args.no_batched:
         out["batched"] = batched_bench(min(args.steps, 20), args.warmup, dev, rank)
+    if world == 1 and not args.no_configs:
+        out["configs"] = configs_bench(dev, flush)
     if world == 1 and not args.no_cpu_baseline and args.reps == 64:
         out["cpu_baseline"] = cpu_baseline()
     print(json.dumps(out), flush=True)

@@ -8,14 +8,18 @@
 // dL/dd per pair, with g = dL/dD + (dL/dd) D / d:
 //     dL/dr_i -= g,   dL/dr_j += g,   dL/dcell[m][k] += c_m g_k.
 //
-// i-side: pairs are sorted by i, so each atom's row is contiguous and a warp
-// reduces it without atomics.  j-side: FP64 atomicAdd (fast), or, when
-// deterministic, a stable radix sort of the pairs by j followed by the same
-// per-atom segmented reduction.  Cell: per-CTA partial sums reduced in a fixed
-// order.  With `deterministic` every result is bit-reproducible run to run.
+// Default: one thread per pair (a flat, fully coalesced pass over the pairs);
+// the i-side sums each warp's runs of equal i with a segmented shuffle scan
+// and adds one FP64 atomic per run, the j-side adds FP64 atomics per pair.
+// Deterministic: pairs are sorted by i, so each atom's row is contiguous and
+// a warp reduces it without atomics; the j-side is a stable radix sort of the
+// pairs by j followed by the same per-atom reduction.  Cell: per-CTA partial
+// sums reduced in a fixed order.  With `deterministic` every result is
+// bit-reproducible run to run.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -129,6 +133,74 @@ k_bwd_rows(PairGrad pg, const int64_t *__restrict__ off, int64_t nat,
     }
 }
 
+// Default path: thread per pair.  grad_pos must be zeroed; receives
+// sum_j-side g - sum_i-side g through FP64 atomics.
+__global__ void __launch_bounds__(kBwdThreads)
+k_bwd_pairs(PairGrad pg, const int32_t *__restrict__ first,
+            const int32_t *__restrict__ second, const int32_t *__restrict__ shift, int64_t P,
+            int pbc_bits, double *__restrict__ grad_pos, double *__restrict__ cell_part) {
+    __shared__ double s_cell[kBwdWarps][9];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double c[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) c[k] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * kBwdThreads;
+    for (int64_t base = (int64_t)blockIdx.x * kBwdThreads + warp * 32; base < P;
+         base += stride) {
+        const int64_t p = base + lane;
+        const bool act = p < P;
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        int i = -1;
+        if (act) {
+            pg.at(p, g0, g1, g2);
+            i = first[p];
+            const int64_t j = second[p];
+            const double s0 = (pbc_bits & 1) ? (double)shift[3 * p + 0] : 0.0;
+            const double s1 = (pbc_bits & 2) ? (double)shift[3 * p + 1] : 0.0;
+            const double s2 = (pbc_bits & 4) ? (double)shift[3 * p + 2] : 0.0;
+            c[0] += s0 * g0; c[1] += s0 * g1; c[2] += s0 * g2;
+            c[3] += s1 * g0; c[4] += s1 * g1; c[5] += s1 * g2;
+            c[6] += s2 * g0; c[7] += s2 * g1; c[8] += s2 * g2;
+            atomicAdd(grad_pos + 3 * j + 0, g0);
+            atomicAdd(grad_pos + 3 * j + 1, g1);
+            atomicAdd(grad_pos + 3 * j + 2, g2);
+        }
+        // runs of equal i are contiguous: segmented inclusive scan over lanes
+        double r0 = g0, r1 = g1, r2 = g2;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double t0 = __shfl_up_sync(full, r0, d);
+            const double t1 = __shfl_up_sync(full, r1, d);
+            const double t2 = __shfl_up_sync(full, r2, d);
+            const int ii = __shfl_up_sync(full, i, d);
+            if (lane >= d && ii == i) {
+                r0 += t0;
+                r1 += t1;
+                r2 += t2;
+            }
+        }
+        const int inext = __shfl_down_sync(full, i, 1);
+        if (act && (lane == 31 || inext != i)) {
+            atomicAdd(grad_pos + 3 * (int64_t)i + 0, -r0);
+            atomicAdd(grad_pos + 3 * (int64_t)i + 1, -r1);
+            atomicAdd(grad_pos + 3 * (int64_t)i + 2, -r2);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) c[k] = warp_sum(c[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) s_cell[warp][k] = c[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        double t = 0.0;
+        for (int w = 0; w < kBwdWarps; w++) t += s_cell[w][threadIdx.x];
+        cell_part[9 * blockIdx.x + threadIdx.x] = t;
+    }
+}
+
 // j-side in deterministic order: perm lists the pairs sorted by j (stable).
 __global__ void __launch_bounds__(kBwdThreads)
 k_bwd_cols(PairGrad pg, const int64_t *__restrict__ coff, const int32_t *__restrict__ perm,
@@ -162,13 +234,59 @@ __global__ void k_bwd_combine(const double *__restrict__ gi, const double *__res
     if (t < n3) out[t] = gj[t] - gi[t];
 }
 
-__global__ void k_bwd_cell(const double *__restrict__ part, int nblocks,
-                           double *__restrict__ grad_cell) {
-    const int k = threadIdx.x;
-    if (k >= 9) return;
-    double t = 0.0;
-    for (int b = 0; b < nblocks; b++) t += part[9 * b + k];
-    grad_cell[k] = t;
+// Sum of the per-CTA cell partials in a fixed order: thread t of one block
+// takes partials t, t + blockDim, ...; then a fixed tree over the threads.
+__global__ void __launch_bounds__(kBwdThreads)
+k_bwd_cell(const double *__restrict__ part, int nblocks, double *__restrict__ grad_cell) {
+    __shared__ double s[kBwdThreads][9];
+    double t[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) t[k] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += kBwdThreads) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) t[k] += part[9 * b + k];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) s[threadIdx.x][k] = t[k];
+    __syncthreads();
+    for (int h = kBwdThreads / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) s[threadIdx.x][k] += s[threadIdx.x + h][k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 9) grad_cell[threadIdx.x] = s[0][threadIdx.x];
+}
+
+// Stream-ordered scratch comes from a pool of this library's own per device
+// that keeps its memory between calls (the default pool would hand it back to
+// the driver at every synchronisation and map it again on the next call).
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
+cudaError_t scratch_pool(int dev, cudaMemPool_t *pool) {
+    if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        g_pools[dev] = p;
+    }
+    *pool = g_pools[dev];
+    return cudaSuccess;
 }
 
 __global__ void k_iota_keys(const int32_t *__restrict__ second, int64_t n,
@@ -206,9 +324,12 @@ extern "C" NBL_API nbl_status nbl_backward(const nbl_backward_args *g, void *str
     int nsm = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int rows_grid = (int)std::max<int64_t>(1, std::min<int64_t>((N + kBwdWarps - 1) /
-                                                                           kBwdWarps,
-                                                                       (int64_t)nsm * 8));
+    const int rows_grid =
+        g->deterministic
+            ? (int)std::max<int64_t>(1, std::min<int64_t>((N + kBwdWarps - 1) / kBwdWarps,
+                                                          (int64_t)nsm * 8))
+            : (int)std::max<int64_t>(1, std::min<int64_t>((P + kBwdThreads - 1) / kBwdThreads,
+                                                          (int64_t)nsm * 8));
     const int pbc_bits = (g->pbc && g->pbc[0] ? 1 : 0) | (g->pbc && g->pbc[1] ? 2 : 0) |
                          (g->pbc && g->pbc[2] ? 4 : 0);
     PairGrad pg{g->grad_distvec, g->grad_absdist, g->distvec, g->absdist};
@@ -238,13 +359,18 @@ extern "C" NBL_API nbl_status nbl_backward(const nbl_backward_args *g, void *str
         o_coff = add(sizeof(int64_t) * (N + 1));
     }
     {
-        NBL_CUDA(cudaMallocAsync((void **)&scratch, std::max<size_t>(bytes, 256), st),
+        cudaMemPool_t pool = nullptr;
+        NBL_CUDA(scratch_pool(dev, &pool), "backward scratch pool");
+        NBL_CUDA(cudaMallocFromPoolAsync((void **)&scratch, std::max<size_t>(bytes, 256), pool,
+                                         st),
                  "backward scratch");
         int64_t *off = reinterpret_cast<int64_t *>(scratch + o_off);
         double *gi = reinterpret_cast<double *>(scratch + o_gi);
         double *gj = reinterpret_cast<double *>(scratch + o_gj);
         double *cell_part = reinterpret_cast<double *>(scratch + o_cell);
-        if (g->row_offsets) {
+        if (!g->deterministic) {
+            // the default path reads no row offsets
+        } else if (g->row_offsets) {
             NBL_CUDA(cudaMemcpyAsync(off, g->row_offsets, sizeof(int64_t) * (N + 1),
                                      cudaMemcpyDeviceToDevice, st), "row offsets");
         } else {
@@ -252,13 +378,21 @@ extern "C" NBL_API nbl_status nbl_backward(const nbl_backward_args *g, void *str
             count_launch();
             NBL_CUDA(cudaGetLastError(), "row starts");
         }
-        NBL_CUDA(cudaMemsetAsync(gj, 0, sizeof(double) * 3 * std::max<int64_t>(N, 1), st),
-                 "memset");
-        k_bwd_rows<<<rows_grid, kBwdThreads, 0, st>>>(pg, off, N, g->shift, g->second, pbc_bits,
-                                                      gi, g->deterministic ? nullptr : gj,
-                                                      cell_part);
-        count_launch();
-        NBL_CUDA(cudaGetLastError(), "backward rows");
+        if (!g->deterministic) {
+            NBL_CUDA(cudaMemsetAsync(g->grad_positions, 0,
+                                     sizeof(double) * 3 * std::max<int64_t>(N, 1), st),
+                     "memset");
+            k_bwd_pairs<<<rows_grid, kBwdThreads, 0, st>>>(pg, g->first, g->second, g->shift,
+                                                           P, pbc_bits, g->grad_positions,
+                                                           cell_part);
+            count_launch();
+            NBL_CUDA(cudaGetLastError(), "backward pairs");
+        } else {
+            k_bwd_rows<<<rows_grid, kBwdThreads, 0, st>>>(pg, off, N, g->shift, g->second,
+                                                          pbc_bits, gi, nullptr, cell_part);
+            count_launch();
+            NBL_CUDA(cudaGetLastError(), "backward rows");
+        }
         if (g->deterministic && P > 0) {
             uint32_t *keys = reinterpret_cast<uint32_t *>(scratch + o_keys);
             int32_t *vals = reinterpret_cast<int32_t *>(scratch + o_vals);
@@ -286,13 +420,13 @@ extern "C" NBL_API nbl_status nbl_backward(const nbl_backward_args *g, void *str
             count_launch();
             NBL_CUDA(cudaGetLastError(), "backward columns");
         }
-        if (N > 0) {
+        if (N > 0 && g->deterministic) {
             k_bwd_combine<<<(unsigned)((3 * N + 255) / 256), 256, 0, st>>>(gi, gj, 3 * N,
                                                                            g->grad_positions);
             count_launch();
             NBL_CUDA(cudaGetLastError(), "combine");
         }
-        k_bwd_cell<<<1, 32, 0, st>>>(cell_part, rows_grid, g->grad_cell);
+        k_bwd_cell<<<1, kBwdThreads, 0, st>>>(cell_part, rows_grid, g->grad_cell);
         count_launch();
         NBL_CUDA(cudaGetLastError(), "cell gradient");
     }
