@@ -776,17 +776,39 @@ k_count(TraverseArgs a) {
                                 cnt[g] = 0;
                                 mw[g] = 0u;
                             }
+                            // atoms in pairs for the packed (f32x2) arithmetic:
+                            // x - p == x + (-p) exactly, and the packed ops round
+                            // each half like the scalar fmaf chain
+                            constexpr int kHalf = GROUP / 2;
+                            float2 nx[kHalf], ny[kHalf], nz[kHalf];
+#pragma unroll
+                            for (int h = 0; h < kHalf; h++) {
+                                nx[h] = make_float2(-pg[2 * h].x, -pg[2 * h + 1].x);
+                                ny[h] = make_float2(-pg[2 * h].y, -pg[2 * h + 1].y);
+                                nz[h] = make_float2(-pg[2 * h].z, -pg[2 * h + 1].z);
+                            }
                             for (int ch = 0; ch < nck; ch++) {
                                 const int k = ch * 32 + lane;
                                 const float4 cv = sm.cand[k];
                                 unsigned m[GROUP];
                                 bool amb_any = false, amb[GROUP];
+                                float r2g[GROUP];
+                                const float2 cx = make_float2(cv.x, cv.x);
+                                const float2 cy = make_float2(cv.y, cv.y);
+                                const float2 cz = make_float2(cv.z, cv.z);
+#pragma unroll
+                                for (int h = 0; h < kHalf; h++) {
+                                    const float2 dx = __fadd2_rn(cx, nx[h]);
+                                    const float2 dy = __fadd2_rn(cy, ny[h]);
+                                    const float2 dz = __fadd2_rn(cz, nz[h]);
+                                    const float2 r2 =
+                                        __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                    r2g[2 * h] = r2.x;
+                                    r2g[2 * h + 1] = r2.y;
+                                }
 #pragma unroll
                                 for (int g = 0; g < GROUP; g++) {
-                                    const float dx = cv.x - pg[g].x;
-                                    const float dy = cv.y - pg[g].y;
-                                    const float dz = cv.z - pg[g].z;
-                                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                                    const float r2 = r2g[g];
                                     float lo, hi;
                                     thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
                                     const bool notself = k != ks[g];

@@ -8,7 +8,8 @@
 //
 // Scan: three-phase (tile reduce -> recursive scan of tile sums -> tile scan
 // with carry-in); no inter-block waiting, so no spin loops at all.
-// Sort: 8-bit digits; per pass one histogram kernel, one scan of the
+// Sort: as few passes as digits of up to 10 bits allow (a 17-bit dense cell
+// key takes two passes of 9 bits); per pass one histogram kernel, one scan of the
 // digit-major histogram and one stable scatter kernel.  Stability (needed so
 // that the atoms of one cell stay in ascending index order, exactly as the
 // reference's counting sort leaves them) comes from ranking keys in index
@@ -166,33 +167,39 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortIters = 16;                               // per warp
 constexpr int kSortTile = kSortThreads * kSortIters;         // 4096
-constexpr int kRadix = 256;
+constexpr int kDigitMax = 10;                 // bits per pass (at most)
+constexpr int kRadix = 1 << kDigitMax;        // bins of the widest pass
 
+// Per-tile digit histogram; `nb` = 1 << digit bits of this pass.
 __global__ void __launch_bounds__(kSortThreads)
-k_radix_hist(const uint32_t *__restrict__ keys, int64_t n, int shift,
+k_radix_hist(const uint32_t *__restrict__ keys, int64_t n, int shift, int nb,
              int32_t *__restrict__ hist, int ntiles) {
     __shared__ int32_t s_cnt[kRadix];
-    s_cnt[threadIdx.x] = 0;
+    for (int d = threadIdx.x; d < nb; d += kSortThreads) s_cnt[d] = 0;
     __syncthreads();
+    const uint32_t mask = (uint32_t)nb - 1u;
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
 #pragma unroll 4
     for (int it = 0; it < kSortIters; it++) {
         int64_t idx = base + (int64_t)it * kSortThreads + threadIdx.x;
-        if (idx < n) atomicAdd(&s_cnt[(keys[idx] >> shift) & 0xffu], 1);
+        if (idx < n) atomicAdd(&s_cnt[(keys[idx] >> shift) & mask], 1);
     }
     __syncthreads();
-    hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = s_cnt[threadIdx.x];
+    for (int d = threadIdx.x; d < nb; d += kSortThreads)
+        hist[(int64_t)d * ntiles + blockIdx.x] = s_cnt[d];
 }
 
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_scatter(const uint32_t *__restrict__ kin, const int32_t *__restrict__ vin,
                 uint32_t *__restrict__ kout, int32_t *__restrict__ vout, int64_t n,
-                int shift, const int32_t *__restrict__ hoff, int ntiles) {
+                int shift, int nb, const int32_t *__restrict__ hoff, int ntiles) {
     __shared__ int32_t s_wc[kSortWarps][kRadix];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads)
-        (&s_wc[0][0])[i] = 0;
+    for (int d = threadIdx.x; d < nb; d += kSortThreads)
+#pragma unroll
+        for (int w = 0; w < kSortWarps; w++) s_wc[w][d] = 0;
     __syncthreads();
+    const uint32_t mask = (uint32_t)nb - 1u;
 
     const unsigned lt = (1u << lane) - 1u;
     const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortIters);
@@ -206,7 +213,7 @@ k_radix_scatter(const uint32_t *__restrict__ kin, const int32_t *__restrict__ vi
         key[it] = valid ? kin[idx] : 0u;
         val[it] = valid ? vin[idx] : 0;
         // Invalid lanes get a private pseudo-digit so they never match.
-        const uint32_t d = valid ? ((key[it] >> shift) & 0xffu) : (kRadix + lane);
+        const uint32_t d = valid ? ((key[it] >> shift) & mask) : (kRadix + lane);
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         int r = 0;
         if (valid) r = s_wc[warp][d] + __popc(peers & lt);
@@ -217,8 +224,7 @@ k_radix_scatter(const uint32_t *__restrict__ kin, const int32_t *__restrict__ vi
     }
     __syncthreads();
     // Exclusive prefix over warps, per digit.
-    {
-        const int d = threadIdx.x;
+    for (int d = threadIdx.x; d < nb; d += kSortThreads) {
         int32_t run = 0;
 #pragma unroll
         for (int w = 0; w < kSortWarps; w++) {
@@ -232,7 +238,7 @@ k_radix_scatter(const uint32_t *__restrict__ kin, const int32_t *__restrict__ vi
     for (int it = 0; it < kSortIters; it++) {
         const int64_t idx = wbase + it * 32 + lane;
         if (idx < n) {
-            const uint32_t d = (key[it] >> shift) & 0xffu;
+            const uint32_t d = (key[it] >> shift) & mask;
             const int64_t pos = (int64_t)hoff[(int64_t)d * ntiles + blockIdx.x] +
                                 s_wc[warp][d] + rank[it];
             kout[pos] = key[it];
@@ -258,15 +264,18 @@ cudaError_t radix_sort_pairs(uint32_t *keys, int32_t *vals, uint32_t *keys_alt,
     const int ntiles = (int)((n + kSortTile - 1) / kSortTile);
     uint32_t *ka = keys, *kb = keys_alt;
     int32_t *va = vals, *vb = vals_alt;
-    for (int shift = 0; shift < bits; shift += 8) {
-        k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(ka, n, shift, hist, ntiles);
+    // As few passes as digits of at most kDigitMax bits allow, of equal width.
+    const int passes = (bits + kDigitMax - 1) / kDigitMax;
+    const int digit = (bits + passes - 1) / passes;
+    const int nb = 1 << digit;
+    for (int shift = 0; shift < bits; shift += digit) {
+        k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(ka, n, shift, nb, hist, ntiles);
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        e = exclusive_scan_i32_i32(hist, (int64_t)ntiles * kRadix, hist_scan,
-                                   scan_scratch, st);
+        e = exclusive_scan_i32_i32(hist, (int64_t)ntiles * nb, hist_scan, scan_scratch, st);
         if (e != cudaSuccess) return e;
-        k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(ka, va, kb, vb, n, shift,
+        k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(ka, va, kb, vb, n, shift, nb,
                                                          hist_scan, ntiles);
         count_launch();
         e = cudaGetLastError();
