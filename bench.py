@@ -352,6 +352,60 @@ def configs_bench(dev, flush, reps=10):
                     "ms": bt * 1e3, "achieved_gbs": alg / bt / 1e9,
                     "frac": alg / bt / 1e9 / peak, "peak_gbs": peak,
                     "peak_source": peak_kind, "algorithmic_bytes": alg}
+        if name.startswith("C5"):
+            # CSR helpers on the device: row starts, then the triplets of pairs
+            # shorter than 3.5 A (the first shell) -- against the reference's
+            # own first_neighbours / triplet_list on the host (serial code)
+            tcut = 3.5
+            seed = torch.empty(nat + 1, dtype=torch.int32, device=dev)
+            dt = bufs["d"]
+            n3 = ctypes.c_int64()
+            fms, tms = [], []
+            for k in range(reps + 3):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e2 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(dev)
+                e0.record(stream)
+                ext.check(ext.lib.nbl_first_neighbours(nat, npairs,
+                                                       ctypes.c_void_p(bufs["i"].data_ptr()),
+                                                       ctypes.c_void_p(seed.data_ptr()), sptr))
+                e1.record(stream)
+                ext.check(ext.lib.nbl_triplet_list(nat + 1, ctypes.c_void_p(seed.data_ptr()),
+                                                   ctypes.c_void_p(dt.data_ptr()), tcut, None,
+                                                   None, 0, ctypes.byref(n3), sptr))
+                if k == 0:
+                    tij = torch.empty(n3.value, dtype=torch.int32, device=dev)
+                    tik = torch.empty(n3.value, dtype=torch.int32, device=dev)
+                ext.check(ext.lib.nbl_triplet_list(nat + 1, ctypes.c_void_p(seed.data_ptr()),
+                                                   ctypes.c_void_p(dt.data_ptr()), tcut,
+                                                   ctypes.c_void_p(tij.data_ptr()),
+                                                   ctypes.c_void_p(tik.data_ptr()), n3.value,
+                                                   ctypes.byref(n3), sptr))
+                e2.record(stream)
+                e2.synchronize()
+                if k >= 3:
+                    fms.append(e0.elapsed_time(e1))
+                    tms.append(e1.elapsed_time(e2))
+            seed_h = seed.cpu().numpy()
+            d_h = dt.cpu().numpy()
+            ct = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                if have_ref:
+                    O.ref_first_neighbours(nat, bufs["i"].cpu().numpy())
+                    O.ref_triplet_list(seed_h, d_h, tcut)
+                else:
+                    O.oracle_first_neighbours(nat, bufs["i"].cpu().numpy())
+                    O.oracle_triplet_list(seed_h, d_h, tcut)
+                ct.append(time.perf_counter() - t0)
+            row["csr_helpers"] = {
+                "first_neighbours_ms": statistics.median(fms),
+                "triplet_list_ms": statistics.median(tms),
+                "triplet_cutoff_A": tcut, "ntriplets": int(n3.value),
+                "note": "triplet_list = count call + fill call (each synchronises once)",
+                "cpu_ms": 1e3 * statistics.median(ct),
+                "cpu": {"kind": "reference" if have_ref else "port", "cores": 1}}
         out[name] = row
     return out
 

@@ -292,6 +292,28 @@ typedef struct nbl_backward_args {
 
 NBL_API nbl_status nbl_backward(const nbl_backward_args *args, void *stream);
 
+/* ---- CSR helpers of a pair list, on the device --------------------------- */
+
+/* Row starts of an i-sorted pair list (all pointers device memory):
+   seed[k], k in [0, n], is the first pair of atom k; -1 before the first atom
+   with pairs, npairs after the last; an empty row gets the next row's start.
+   Asynchronous on `stream`.  Replaces first_neighbours()
+   (src/libneighbours/first_neighbours.cc:15-38). */
+NBL_API nbl_status nbl_first_neighbours(int64_t n, int64_t npairs, const int32_t *first,
+                                        int32_t *seed, void *stream);
+
+/* Triplets of pairs sharing a first atom, from row starts first_i[nfirst]
+   (device memory): for each row, every ordered (ij, ik), ij != ik, ij major;
+   with absdist (device, may be NULL) only pairs with absdist < cutoff take
+   part.  Sets *ntriplets (synchronises `stream`); writes ij/ik (device,
+   `capacity` entries) when both are given, NBL_ERROR_CAPACITY if they are too
+   short.  Call with ij = ik = NULL to size the outputs.  Replaces
+   triplet_list() (src/libneighbours/triplet_list.cc:15-34). */
+NBL_API nbl_status nbl_triplet_list(int64_t nfirst, const int32_t *first_i,
+                                    const double *absdist, double cutoff, int32_t *ij,
+                                    int32_t *ik, int64_t capacity, int64_t *ntriplets,
+                                    void *stream);
+
 /* Allocation-free variant of nbl_count + nbl_fill, for callers that cannot
    allocate device memory at call time (an MD loop that forbids allocation
    after start-up, a host whose pool allocator has reserved the device

@@ -259,12 +259,24 @@ k_bwd_cell(const double *__restrict__ part, int nblocks, double *__restrict__ gr
     if (threadIdx.x < 9) grad_cell[threadIdx.x] = s[0][threadIdx.x];
 }
 
+__global__ void k_iota_keys(const int32_t *__restrict__ second, int64_t n,
+                            uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    keys[p] = (uint32_t)second[p];
+    vals[p] = (int32_t)p;
+}
+
+}  // namespace
+
 // Stream-ordered scratch comes from a pool of this library's own per device
 // that keeps its memory between calls (the default pool would hand it back to
 // the driver at every synchronisation and map it again on the next call).
+namespace {
 constexpr int kMaxPoolDevices = 64;
 std::mutex g_pool_mutex;
 cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+}  // namespace
 
 cudaError_t scratch_pool(int dev, cudaMemPool_t *pool) {
     if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
@@ -288,16 +300,6 @@ cudaError_t scratch_pool(int dev, cudaMemPool_t *pool) {
     *pool = g_pools[dev];
     return cudaSuccess;
 }
-
-__global__ void k_iota_keys(const int32_t *__restrict__ second, int64_t n,
-                            uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    keys[p] = (uint32_t)second[p];
-    vals[p] = (int32_t)p;
-}
-
-}  // namespace
 
 }  // namespace nbl
 

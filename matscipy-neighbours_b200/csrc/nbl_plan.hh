@@ -101,6 +101,10 @@ struct Plan {
     bool stage_in_flight = false;
 };
 
+// Stream-ordered scratch pool of device `dev` that keeps its memory between
+// calls (cudaMallocFromPoolAsync / cudaFreeAsync on it).
+cudaError_t scratch_pool(int dev, cudaMemPool_t *pool);
+
 nbl_status set_error(nbl_status st, const char *fmt, ...);
 nbl_status cuda_status(cudaError_t e, const char *where);
 nbl_status plan_system(const double origin[3], const double cell[9],

@@ -95,6 +95,9 @@ def _load():
         "nbl_device_type": ([], ctypes.c_int),
         "nbl_version": ([], ctypes.c_char_p),
         "nbl_launch_count": ([ctypes.c_int], ctypes.c_longlong),
+        "nbl_first_neighbours": ([ctypes.c_int64, ctypes.c_int64, P, P, P], ctypes.c_int),
+        "nbl_triplet_list": ([ctypes.c_int64, P, P, ctypes.c_double, P, P, ctypes.c_int64,
+                              ctypes.POINTER(ctypes.c_int64), P], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -547,10 +550,44 @@ def neighbour_matrix_dlpack(cell_origin, cell, inv_cell, pbc, host_pos, cutoffs,
 # the GPU hot path.
 # ---------------------------------------------------------------------------
 
+def _device_array(x, dtype):
+    """A torch CUDA tensor of `dtype` viewing (or, for another dtype, copying)
+    a device array `x` (torch tensor or anything with a CUDA __dlpack__);
+    None for host arrays."""
+    dev = getattr(x, "__dlpack_device__", None)
+    if dev is None:
+        return None
+    try:
+        if int(dev()[0]) == 1:  # kDLCPU
+            return None
+    except Exception:
+        return None
+    torch = _torch()
+    t = x if isinstance(x, torch.Tensor) else torch.from_dlpack(x)
+    if not t.is_cuda:
+        return None
+    return t.to(dtype).contiguous()
+
+
 def first_neighbours(n, i):
     """seed[k] = index of the first pair of atom k in the i-sorted list,
-    seed[n] = len(i); -1 for atoms before the first one with pairs."""
+    seed[n] = len(i); -1 for atoms before the first one with pairs.  A device
+    `i` (torch CUDA tensor or CUDA __dlpack__) is handled on its GPU and
+    gives a torch CUDA tensor."""
     n = int(n)
+    it = _device_array(i, _torch().int32) if hasattr(i, "__dlpack_device__") else None
+    if it is not None:
+        torch = _torch()
+        if it.dim() != 1:
+            raise ValueError("object too deep for desired array")
+        seed = torch.empty(n + 1, dtype=torch.int32, device=it.device)
+        stream = torch.cuda.current_stream(it.device)
+        with torch.cuda.device(it.device):
+            check(lib.nbl_first_neighbours(n, int(it.shape[0]),
+                                           ctypes.c_void_p(it.data_ptr()) if it.numel() else None,
+                                           ctypes.c_void_p(seed.data_ptr()),
+                                           ctypes.c_void_p(stream.cuda_stream)))
+        return seed
     i = _fromany(i, np.int32, 1, 1)
     nn = i.shape[0]
     if nn == 0:
@@ -573,6 +610,10 @@ def get_jump_indicies(sorted_array):
 def triplet_list(first_i, absdist=None, cutoff=None):
     """(ij, ik) pair-index triplets sharing a first atom, ij != ik, ij-major;
     with distances, both below `cutoff`."""
+    ft = (_device_array(first_i, _torch().int32)
+          if hasattr(first_i, "__dlpack_device__") else None)
+    if ft is not None:
+        return _triplet_list_device(ft, absdist, cutoff)
     fn = _fromany(first_i, np.int32, 1, 1)
     if absdist is not None and cutoff is None:
         raise TypeError("triplet_list: distances given without a cutoff")
@@ -593,3 +634,34 @@ def triplet_list(first_i, absdist=None, cutoff=None):
     if not ij_all:
         return np.zeros(0, dtype=np.int32), np.zeros(0, dtype=np.int32)
     return np.concatenate(ij_all), np.concatenate(ik_all)
+
+
+def _triplet_list_device(ft, absdist, cutoff):
+    """triplet_list on the GPU of `ft` (nbl_triplet_list): torch CUDA tensors."""
+    torch = _torch()
+    if absdist is not None and cutoff is None:
+        raise TypeError("triplet_list: distances given without a cutoff")
+    dt = None
+    if absdist is not None:
+        dt = _device_array(absdist, torch.float64) if hasattr(absdist, "__dlpack_device__") \
+            else None
+        if dt is None:
+            dt = torch.as_tensor(np.ascontiguousarray(absdist, dtype=np.float64),
+                                 device=ft.device)
+    stream = torch.cuda.current_stream(ft.device)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    fp = ctypes.c_void_p(ft.data_ptr()) if ft.numel() else None
+    dp = ctypes.c_void_p(dt.data_ptr()) if dt is not None and dt.numel() else None
+    c = float(cutoff) if cutoff is not None else 0.0
+    n = ctypes.c_int64()
+    with torch.cuda.device(ft.device):
+        check(lib.nbl_triplet_list(int(ft.shape[0]), fp, dp, c, None, None, 0,
+                                   ctypes.byref(n), sp))
+        ij = torch.empty(int(n.value), dtype=torch.int32, device=ft.device)
+        ik = torch.empty(int(n.value), dtype=torch.int32, device=ft.device)
+        if n.value:
+            check(lib.nbl_triplet_list(int(ft.shape[0]), fp, dp, c,
+                                       ctypes.c_void_p(ij.data_ptr()),
+                                       ctypes.c_void_p(ik.data_ptr()), int(n.value),
+                                       ctypes.byref(n), sp))
+    return ij, ik

@@ -277,7 +277,13 @@ get_jump_indicies = _ext.get_jump_indicies
 
 def triplet_list(first_neighbours, abs_dr_p=None, cutoff=None):
     """Triplet list from a first-neighbour (row-start) array
-    (``neighbours.py:360-370``): distances are used only with a cutoff."""
+    (``neighbours.py:360-370``): distances are used only with a cutoff.  A
+    device array (torch CUDA tensor or CUDA __dlpack__) is handled on its GPU
+    and gives torch CUDA tensors."""
+    if _is_on_device(first_neighbours):
+        if abs_dr_p is not None and cutoff is not None:
+            return _ext.triplet_list(first_neighbours, abs_dr_p, float(cutoff))
+        return _ext.triplet_list(first_neighbours)
     first_neighbours = np.ascontiguousarray(first_neighbours, dtype=np.int32)
     if abs_dr_p is not None and cutoff is not None:
         abs_dr_p = np.ascontiguousarray(abs_dr_p, dtype=float)

@@ -406,3 +406,42 @@ int oracle_neighbour_list(int quantities, const double origin[3],
     free(ty_s);
     return ORACLE_OK;
 }
+
+/* ---- CSR helpers ---------------------------------------------------------- */
+
+/* first_neighbours.cc:15-38. */
+void oracle_first_neighbours(int32_t n, int64_t nn, const int32_t *i, int32_t *seed) {
+    for (int64_t k = 0; k <= n; k++) seed[k] = -1;
+    if (nn <= 0) {
+        for (int64_t k = 0; k <= n; k++) seed[k] = 0;
+        return;
+    }
+    seed[i[0]] = 0;
+    for (int64_t k = 1; k < nn; k++) {
+        if (i[k] != i[k - 1]) {
+            for (int64_t l = (int64_t)i[k - 1] + 1; l <= i[k]; l++) seed[l] = (int32_t)k;
+        }
+    }
+    for (int64_t k = (int64_t)i[nn - 1] + 1; k <= n; k++) seed[k] = (int32_t)nn;
+}
+
+/* triplet_list.cc:15-34: for each row r, every ordered pair (ij, ik) of its
+   entries with ij != ik, both below the cutoff when distances are given. */
+int64_t oracle_triplet_list(int32_t nfirst, const int32_t *first_i, const double *absdist,
+                            double cutoff, int32_t *ij, int32_t *ik, int64_t cap) {
+    int64_t t = 0;
+    for (int32_t r = 0; r < nfirst - 1; r++) {
+        for (int32_t a = first_i[r]; a < first_i[r + 1]; a++) {
+            for (int32_t b = first_i[r]; b < first_i[r + 1]; b++) {
+                if (a == b) continue;
+                if (absdist && (absdist[a] >= cutoff || absdist[b] >= cutoff)) continue;
+                if (ij && ik && t < cap) {
+                    ij[t] = a;
+                    ik[t] = b;
+                }
+                t++;
+            }
+        }
+    }
+    return t;
+}

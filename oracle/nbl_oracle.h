@@ -46,6 +46,16 @@ int oracle_neighbour_list(int quantities, const double origin[3],
 
 void oracle_result_free(oracle_result_t *o);
 
+/* Row starts of an i-sorted pair list (first_neighbours.cc:15-38): seed[k]
+   for k in [0, n]; -1 before the first atom with pairs, nn after the last. */
+void oracle_first_neighbours(int32_t n, int64_t nn, const int32_t *i, int32_t *seed);
+
+/* Triplets (ij, ik) of pairs sharing a first atom (triplet_list.cc:15-34).
+   Returns the triplet count; writes at most `cap` of each when ij/ik are
+   not NULL.  absdist == NULL: no distance filter. */
+int64_t oracle_triplet_list(int32_t nfirst, const int32_t *first_i, const double *absdist,
+                            double cutoff, int32_t *ij, int32_t *ik, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,12 @@ def _load():
         lib = ctypes.CDLL(str(ORACLE_SO))
         lib.oracle_neighbour_list.restype = ctypes.c_int
         lib.oracle_result_free.argtypes = [ctypes.POINTER(_OracleResult)]
+        P = ctypes.c_void_p
+        lib.oracle_first_neighbours.argtypes = [ctypes.c_int32, ctypes.c_int64, P, P]
+        lib.oracle_first_neighbours.restype = None
+        lib.oracle_triplet_list.argtypes = [ctypes.c_int32, P, P, ctypes.c_double, P, P,
+                                            ctypes.c_int64]
+        lib.oracle_triplet_list.restype = ctypes.c_int64
         _lib = lib
     return _lib
 
@@ -101,6 +107,12 @@ def _load_ref():
         lib.ref_set_threads.restype = ctypes.c_int
         lib.ref_set_threads.argtypes = [ctypes.c_int]
         lib.ref_last_error.restype = ctypes.c_char_p
+        P = ctypes.c_void_p
+        lib.ref_first_neighbours.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
+        lib.ref_first_neighbours.restype = None
+        lib.ref_triplet_list.argtypes = [ctypes.c_int, P, P, ctypes.c_double, P, P,
+                                         ctypes.c_int64]
+        lib.ref_triplet_list.restype = ctypes.c_int64
         _ref = lib
     return _ref
 
@@ -272,3 +284,45 @@ def canonical(i, j, S):
     rows = np.column_stack([np.asarray(i), np.asarray(j), np.asarray(S)])
     rows = rows.astype(np.int64)
     return rows[np.lexsort(rows.T[::-1])]
+
+
+# ---- CSR helpers -------------------------------------------------------------
+
+def _csr_first(fn, n, i):
+    i = np.ascontiguousarray(i, dtype=np.int32)
+    seed = np.empty(int(n) + 1, dtype=np.int32)
+    fn(int(n), int(i.shape[0]), i.ctypes.data if i.size else None, seed.ctypes.data)
+    return seed
+
+
+def _csr_triplets(fn, first_i, absdist, cutoff):
+    f = np.ascontiguousarray(first_i, dtype=np.int32)
+    d = None if absdist is None else np.ascontiguousarray(absdist, dtype=np.float64)
+    dp = None if d is None else d.ctypes.data
+    c = float(cutoff) if cutoff is not None else 0.0
+    n = int(fn(int(f.shape[0]), f.ctypes.data, dp, c, None, None, 0))
+    ij = np.empty(n, dtype=np.int32)
+    ik = np.empty(n, dtype=np.int32)
+    if n:
+        fn(int(f.shape[0]), f.ctypes.data, dp, c, ij.ctypes.data, ik.ctypes.data, n)
+    return ij, ik
+
+
+def oracle_first_neighbours(n, i):
+    """first_neighbours.cc:15-38 restated in C (nbl_oracle.c)."""
+    return _csr_first(_load().oracle_first_neighbours, n, i)
+
+
+def oracle_triplet_list(first_i, absdist=None, cutoff=None):
+    """triplet_list.cc:15-34 restated in C (nbl_oracle.c)."""
+    return _csr_triplets(_load().oracle_triplet_list, first_i, absdist, cutoff)
+
+
+def ref_first_neighbours(n, i):
+    """The reference's own first_neighbours (oracle/_ref)."""
+    return _csr_first(_load_ref().ref_first_neighbours, n, i)
+
+
+def ref_triplet_list(first_i, absdist=None, cutoff=None):
+    """The reference's own triplet_list (oracle/_ref)."""
+    return _csr_triplets(_load_ref().ref_triplet_list, first_i, absdist, cutoff)

@@ -21,7 +21,9 @@
 #endif
 
 #include "error.hh"
+#include "first_neighbours.hh"
 #include "neighbour_list.hh"
+#include "triplet_list.hh"
 
 using namespace matscipy;
 
@@ -76,6 +78,26 @@ int ref_neighbour_list(int quantities, const double *origin, const double *cell,
     out->d = dup(nl.absdist);
     out->S = dup(nl.shift);
     return 0;
+}
+
+/* first_neighbours (first_neighbours.hh) on the reference's own code. */
+void ref_first_neighbours(int n, int nn, const int *i, int *seed) {
+    first_neighbours(n, nn, i, seed);
+}
+
+/* triplet_list (triplet_list.hh); returns the count, copies at most cap. */
+int64_t ref_triplet_list(int nfirst, const int *first_i, const double *absdist,
+                         double cutoff, int *ij, int *ik, int64_t cap) {
+    std::vector<index_t> a, b;
+    triplet_list(nfirst, first_i, absdist, cutoff, a, b);
+    const int64_t t = (int64_t)a.size();
+    if (ij && ik) {
+        for (int64_t k = 0; k < t && k < cap; k++) {
+            ij[k] = a[k];
+            ik[k] = b[k];
+        }
+    }
+    return t;
 }
 
 void ref_result_free(ref_result_t *o) {

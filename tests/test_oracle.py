@@ -92,3 +92,40 @@ def test_oracle_equals_reference_core_when_built(oracle):
                                       w["pbc"])
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+
+
+# --- CSR helpers: the oracle's restatement against the reference's own code
+#     (first_neighbours.cc, triplet_list.cc compiled into oracle/_ref) and the
+#     reference tests' known answers (tests/test_extension.py:277-336) ---------
+
+def test_csr_oracle_known_answers(oracle):
+    f = oracle.oracle_first_neighbours
+    assert list(f(5, [1, 1, 1, 1, 3, 3, 3])) == [-1, 0, 4, 4, 7, 7]
+    assert list(f(8, [0, 1, 2, 3, 3, 5, 6])) == [0, 1, 2, 3, 5, 5, 6, 7, 7]
+    assert list(f(5, [])) == [0] * 6
+    first_i = np.array([0, 2, 6, 10], dtype=np.int32)
+    ij, ik = oracle.oracle_triplet_list(first_i, np.array([2.2] * 4 + [3.0] * 2 + [2.0] * 4),
+                                        2.6)
+    assert list(ij) == [0, 1, 2, 3, 6, 6, 6, 7, 7, 7, 8, 8, 8, 9, 9, 9]
+    assert list(ik) == [1, 0, 3, 2, 7, 8, 9, 6, 8, 9, 6, 7, 9, 6, 7, 8]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_csr_oracle_equals_reference_and_host_path(oracle, seed):
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    rng = np.random.default_rng(seed)
+    n = 300
+    pos = rng.uniform(0, 9, size=(n, 3))
+    i, d = oracle.oracle_neighbour_list("id", 9 * np.eye(3), pos, 2.2, (True, False, True))
+    seed_o = oracle.oracle_first_neighbours(n, i)
+    assert np.array_equal(seed_o, ext.first_neighbours(n, i))
+    if oracle.ref_available():
+        assert np.array_equal(seed_o, oracle.ref_first_neighbours(n, i))
+    for cut in (None, 1.7):
+        dd = None if cut is None else d
+        want = oracle.oracle_triplet_list(seed_o, dd, cut)
+        got = ext.triplet_list(seed_o) if cut is None else ext.triplet_list(seed_o, dd, cut)
+        assert np.array_equal(want[0], got[0]) and np.array_equal(want[1], got[1])
+        if oracle.ref_available():
+            ref = oracle.ref_triplet_list(seed_o, dd, cut)
+            assert np.array_equal(want[0], ref[0]) and np.array_equal(want[1], ref[1])
