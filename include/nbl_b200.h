@@ -292,6 +292,23 @@ typedef struct nbl_backward_args {
 
 NBL_API nbl_status nbl_backward(const nbl_backward_args *args, void *stream);
 
+/* ---- fused consumer: Lennard-Jones forces without a pair list ------------ */
+
+/* Forces and energy of a truncated Lennard-Jones pair potential over the
+   request's neighbour pairs, U = 4 eps ((sigma/r)^12 - (sigma/r)^6) for
+   r < cutoff, computed inside the fill pass: no pair is written.  forces
+   (device, 3 * nat doubles, original atom order) receives F_i = -dU/dr_i
+   summed over the pairs of row i; *energy (device, one double) receives
+   sum over pairs of U / 2 per directed pair, i.e. each unordered pair once.
+   Asynchronous on `stream` (no host synchronisation): call nbl_check to see
+   input errors.  The same pair set as nbl_count/nbl_fill, so the forces are
+   those of the reference's pair list (lj_langevin_gpu.cu:59-74, the
+   reference's example, with eps = sigma = 1 and atomics instead of row sums).
+   The request's quantities are ignored. */
+NBL_API nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
+                                 double sigma, double *forces, double *energy,
+                                 void *stream);
+
 /* ---- CSR helpers of a pair list, on the device --------------------------- */
 
 /* Row starts of an i-sorted pair list (all pointers device memory):

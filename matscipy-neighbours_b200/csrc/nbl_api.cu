@@ -237,6 +237,7 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
     size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1));
     size_t o_items = L.add(sizeof(int2) * std::max<int64_t>(N, 1));
+    size_t o_ljp = L.add(sizeof(double) * (size_t)(std::max<int64_t>(N, 1) + N / 1024 + 64));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
     if (st != NBL_SUCCESS) return st;
     char *base = static_cast<char *>(p.ws.base);
@@ -275,6 +276,7 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     B.mask_cap = mask_cap;
     B.home_mask = (long long *)at(o_hmask);
     B.items = (int2 *)at(o_items);
+    B.lj_part = (double *)at(o_ljp);
     return NBL_SUCCESS;
 }
 
@@ -839,6 +841,48 @@ nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
     std::memcpy(&ov, p.host_small + 2, sizeof(int));
     *overflow = ov ? 1 : 0;
     return r;
+}
+
+nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
+                         double sigma, double *forces, double *energy, void *stream) {
+    clear_error();
+    if (!plan || !req || !energy || (!forces && req->nat > 0))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    if (!(std::isfinite(epsilon) && std::isfinite(sigma)))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "epsilon and sigma must be finite");
+    plan->p.have_count = false;
+    Batch b;
+    nbl_status st = batch_from_request(req, b);
+    if (st != NBL_SUCCESS) return st;
+    if (req->device_id >= 0 && req->device_id != plan->p.device)
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "request device %d != plan device %d",
+                         req->device_id, plan->p.device);
+    DeviceGuard g(plan->p.device);
+    if (!g.ok) return set_error(NBL_ERROR_CUDA, "cannot select device %d", plan->p.device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    Plan &p = plan->p;
+    st = run_count(p, b, cs, false);
+    if (st != NBL_SUCCESS) return st;
+    if (b.natoms == 0) {
+        NBL_CUDA(cudaMemsetAsync(energy, 0, sizeof(double), cs), "memset energy");
+        return NBL_SUCCESS;
+    }
+    TraverseArgs ta = p.targs;
+    ta.first = ta.second = nullptr;
+    ta.distvec = ta.absdist = nullptr;
+    ta.shift = nullptr;
+    ta.capacity = 0;
+    ta.lj_force = forces;
+    ta.lj_energy = p.bufs.lj_part;
+    ta.lj_eps4 = 4.0 * epsilon;
+    ta.lj_eps24 = 24.0 * epsilon;
+    ta.lj_sig2 = sigma * sigma;
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, cs),
+             "force pass");
+    NBL_CUDA(launch_lj_energy(p.bufs.lj_part, b.natoms, p.bufs.lj_part + b.natoms, energy,
+                              cs),
+             "energy");
+    return NBL_SUCCESS;
 }
 
 nbl_status nbl_counts(nbl_plan *plan, int32_t *counts, void *stream) {

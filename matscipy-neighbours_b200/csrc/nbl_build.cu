@@ -300,6 +300,7 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
+static_assert(kWarps == kTraverseWarps, "per-warp partial arrays are sized by kTraverseWarps");
 constexpr int kSeg = 32;         // visited offsets per batch (one per lane)
 constexpr int kITile = 32;       // atoms i per i-tile
 constexpr int kWinWords = 256;   // hit words per emission window
@@ -338,7 +339,7 @@ struct __align__(16) CountSmem {
 };
 
 constexpr int kCandTab = 1024;   // candidates with a segment-table entry (fill)
-constexpr int kPosTab = 960;     // pairs per window with a position table (fill)
+constexpr int kPosTab = 704;     // pairs per window with a position table (fill)
 static_assert(kRange <= 8192 && kITile <= 32,
               "position-table entries hold the candidate in 13 bits, the atom in 5");
 
@@ -351,6 +352,7 @@ struct __align__(16) FillSmem {
     int4 iaux[kITile];
     int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     long long icur[kITile];
+    double facc[kITile][4];    // force sink: the tile's force and energy sums
     uint32_t mw[kWinWords];
     int32_t mpre[kWinWords + 1];
     uint32_t ptab[kPosTab];    // window position -> candidate | atom << 13 (small windows)
@@ -986,6 +988,60 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
     }
 }
 
+// Force sink: one round of pairs, all 32 lanes.  Each active lane forms its
+// pair's Lennard-Jones force on atom i from the exact FP64 D (the reference's
+// operation order, as the stored D), U = 4 eps ((sigma/r)^12 - (sigma/r)^6)
+// cut at the list's cutoff, F_i = -24 eps s6 (2 s6 - 1) D / r^2 with
+// s6 = (sigma^2 / r^2)^3 (lj_langevin_gpu.cu:59-74 with eps = sigma = 1); the
+// lanes' forces and energy shares (1/2 U per directed pair) are summed per
+// atom (runs of equal i are contiguous) and the run's last lane adds them to
+// the tile's shared-memory sums.
+template <bool FP32>
+__device__ __forceinline__ void lj_round(FillSmem<FP32> &sm, const TraverseArgs &a,
+                                         const PairWork &w, int lane) {
+    const unsigned full = 0xffffffffu;
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0, e = 0.0;
+    const int il = w.act ? w.il : -1;
+    if (w.act) {
+        const double4 pi = sm.i64[w.il];
+        const int seg = w.seg;
+        const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
+        const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
+        const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
+        const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+        const double ir2 = 1.0 / r2;
+        const double s2 = a.lj_sig2 * ir2;
+        const double s6 = s2 * s2 * s2;
+        const double coef = -a.lj_eps24 * ir2 * s6 * (2.0 * s6 - 1.0);
+        f0 = coef * dx;
+        f1 = coef * dy;
+        f2 = coef * dz;
+        e = 0.5 * a.lj_eps4 * (s6 * s6 - s6);
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double t0 = __shfl_up_sync(full, f0, d);
+        const double t1 = __shfl_up_sync(full, f1, d);
+        const double t2 = __shfl_up_sync(full, f2, d);
+        const double t3 = __shfl_up_sync(full, e, d);
+        const int ii = __shfl_up_sync(full, il, d);
+        if (lane >= d && ii == il) {
+            f0 += t0;
+            f1 += t1;
+            f2 += t2;
+            e += t3;
+        }
+    }
+    const int inext = __shfl_down_sync(full, il, 1);
+    if (il >= 0 && (lane == 31 || inext != il)) {
+        sm.facc[il][0] += f0;
+        sm.facc[il][1] += f1;
+        sm.facc[il][2] += f2;
+        sm.facc[il][3] += e;
+    }
+    __syncwarp();
+}
+
 template <bool FP32, int KIND>
 __global__ void __launch_bounds__(kThreads, 4)
 k_fill(TraverseArgs a) {
@@ -996,6 +1052,7 @@ k_fill(TraverseArgs a) {
     const unsigned full = 0xffffffffu;
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
+    const bool lj = a.lj_force != nullptr;
 
     for (int it = gwarp; it < nitems; it += nwarps) {
         const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
@@ -1027,6 +1084,7 @@ k_fill(TraverseArgs a) {
                     sm.iaux[c2] = ax;
                     sm.isi[c2] = si;
                     sm.icur[c2] = (long long)a.offsets[ax.x];
+                    sm.facc[c2][0] = sm.facc[c2][1] = sm.facc[c2][2] = sm.facc[c2][3] = 0.0;
                 }
                 __syncwarp();
             }
@@ -1121,7 +1179,10 @@ k_fill(TraverseArgs a) {
                             const PairWork nxt = fetch_pair<FP32>(sm, a, nseg, nchunks, nw,
                                                                   nch, inv_nch, kr, a0, carry,
                                                                   P0 + 32 + lane, tab);
-                            store_pair<FP32>(sm, a, H, cur);
+                            if (lj)
+                                lj_round<FP32>(sm, a, cur, lane);
+                            else
+                                store_pair<FP32>(sm, a, H, cur);
                             cur = nxt;
                         }
                         __syncwarp();
@@ -1140,6 +1201,12 @@ k_fill(TraverseArgs a) {
                     const long long deg = end - (long long)a.offsets[ax];
                     a.mat_count[ax] = (int32_t)deg;
                     if (deg > a.mat_k) atomicOr(a.mat_overflow, 1);
+                }
+                if (lj) {
+                    a.lj_force[3 * (long long)ax + 0] = sm.facc[lane][0];
+                    a.lj_force[3 * (long long)ax + 1] = sm.facc[lane][1];
+                    a.lj_force[3 * (long long)ax + 2] = sm.facc[lane][2];
+                    a.lj_energy[ax] = sm.facc[lane][3];
                 }
             }
             __syncwarp();
@@ -1188,6 +1255,41 @@ cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStrea
     k_visit<<<nsys, 64, 0, st>>>(sys, visit);
     count_launch();
     return cudaGetLastError();
+}
+
+// Fixed-order sum of n values: block b sums values [2048 b, 2048 b + 2048)
+// (thread t: 8 consecutive values, then a fixed tree) into part2[b]; one
+// block then sums the block sums the same way.  The same bits every run.
+__global__ void __launch_bounds__(256) k_sum_fixed(const double *__restrict__ v, int64_t n,
+                                                   double *__restrict__ out) {
+    __shared__ double s[256];
+    const int64_t b0 = (int64_t)blockIdx.x * 2048 + (int64_t)threadIdx.x * 8;
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (b0 + k < n) t += v[b0 + k];
+    s[threadIdx.x] = t;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, double *out,
+                             cudaStream_t st) {
+    const int64_t nb = (n + 2047) / 2048;
+    if (nb <= 1) {
+        k_sum_fixed<<<1, 256, 0, st>>>(atom_e, n, out);
+        count_launch();
+        return cudaGetLastError();
+    }
+    k_sum_fixed<<<(unsigned)nb, 256, 0, st>>>(atom_e, n, scratch);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_lj_energy(scratch, nb, scratch + nb, out, st);
 }
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st) {

@@ -87,6 +87,13 @@ struct TraverseArgs {
     double *mat_dist;
     int32_t *mat_count;
     int *mat_overflow;
+    // Force sink (lj_force != nullptr): instead of writing pairs, the fill
+    // pass sums Lennard-Jones forces per atom i into lj_force[3 * atom] and
+    // its energy share (1/2 U per pair of its row) into lj_energy[atom];
+    // every in-range atom is written once.
+    double *lj_force;
+    double *lj_energy;
+    double lj_eps4, lj_eps24, lj_sig2;
     int *err;
     // Rows produced: only atoms whose global index lies in [i_lo, i_hi) act
     // as i; every atom stays a candidate j.  Rows outside keep count 0.
@@ -96,6 +103,14 @@ struct TraverseArgs {
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
+// Warps per CTA of the pair passes (sizes per-warp partial arrays).
+constexpr int kTraverseWarps = 4;
+
+// Sum of n per-atom energies in a fixed order into *out (one double);
+// scratch holds at least n / 2048 + n / 2048^2 + 2 doubles.
+cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, double *out,
+                             cudaStream_t st);
+
 // Fill the visit tables of the systems that have one (visit_base >= 0).
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,

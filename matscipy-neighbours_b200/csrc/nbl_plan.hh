@@ -60,6 +60,7 @@ struct Bufs {
     long long mask_cap = 0;
     long long *home_mask = nullptr;
     int2 *items = nullptr;
+    double *lj_part = nullptr;     // force sink: per-atom energies, then block sums
 };
 
 struct Workspace {

@@ -17,6 +17,7 @@ from .neighbours import (
     triplet_list,
 )
 from ._matscipy_neighbours import set_options
+from .consumers import lennard_jones
 
 __all__ = [
     "neighbour_list",
@@ -28,4 +29,5 @@ __all__ = [
     "coordination",
     "DLPackTensor",
     "set_options",
+    "lennard_jones",
 ]

@@ -96,6 +96,8 @@ def _load():
         "nbl_version": ([], ctypes.c_char_p),
         "nbl_launch_count": ([ctypes.c_int], ctypes.c_longlong),
         "nbl_first_neighbours": ([ctypes.c_int64, ctypes.c_int64, P, P, P], ctypes.c_int),
+        "nbl_lj_forces": ([P, ctypes.POINTER(Request), ctypes.c_double, ctypes.c_double, P, P,
+                           P], ctypes.c_int),
         "nbl_triplet_list": ([ctypes.c_int64, P, P, ctypes.c_double, P, P, ctypes.c_int64,
                               ctypes.POINTER(ctypes.c_int64), P], ctypes.c_int),
     }
