@@ -407,6 +407,61 @@ def configs_bench(dev, flush, reps=10):
                 "cpu_ms": 1e3 * statistics.median(ct),
                 "cpu": {"kind": "reference" if have_ref else "port", "cores": 1}}
         out[name] = row
+
+    # The fused consumer on the reference's molecular-dynamics benchmark
+    # system: LJ forces and energy of a 1,000,000-atom FCC droplet (reduced
+    # units, lattice 1.6, cutoff 2.5, open box) with no pair list written
+    # (nbl_lj_forces), against the reference's CPU core building the pair
+    # list (all host threads) plus float64 numpy force sums.
+    w = W.lj_droplet()
+    nat = w["positions"].shape[0]
+    cell = np.ascontiguousarray(w["cell"], dtype=float)
+    inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+    pbc8 = np.zeros(3, dtype=np.uint8)
+    pos = torch.from_numpy(w["positions"]).to(dev)
+    req = ext.make_request(ext.QUANTITY_FIRST, np.zeros(3), cell, inv, pbc8, nat,
+                           ctypes.c_void_p(pos.data_ptr()), True, w["cutoff"], None, None,
+                           0, None, dev.index)
+    forces = torch.empty((nat, 3), dtype=torch.float64, device=dev)
+    energy = torch.empty((), dtype=torch.float64, device=dev)
+    evs = []
+    for k in range(reps + 3):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ext.check(ext.lib.nbl_lj_forces(plan, ctypes.byref(req), 1.0, 1.0,
+                                        ctypes.c_void_p(forces.data_ptr()),
+                                        ctypes.c_void_p(energy.data_ptr()), sptr))
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ext.check(ext.lib.nbl_check(plan, sptr))
+    gms = statistics.median([e0.elapsed_time(e1) for e0, e1 in evs[3:]])
+    n = ctypes.c_int64()
+    ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
+
+    def cpu_lj():
+        i, D, d = cpu_fn("iDd", w["cell"], w["positions"], w["cutoff"], w["pbc"])
+        s6 = (1.0 / (d * d)) ** 3
+        coef = -24.0 * s6 * (2.0 * s6 - 1.0) / (d * d)
+        f = np.stack([np.bincount(i, weights=coef * D[:, k], minlength=nat)
+                      for k in range(3)], axis=1)
+        return 0.5 * float(np.sum(4.0 * (s6 * s6 - s6))), f
+
+    t0 = time.perf_counter()
+    e_cpu, f_cpu = cpu_lj()
+    cpu_s = time.perf_counter() - t0
+    out["LJ_droplet_1M"] = {
+        "natoms": nat, "npairs": int(n.value), "cutoff": w["cutoff"],
+        "gpu_ms": gms, "gpu_pairs_per_s": n.value / (gms * 1e-3),
+        "what": "nbl_lj_forces: bin + count + force pass, no pairs written",
+        "energy_rel_diff_vs_cpu": abs(float(energy.item()) - e_cpu) / abs(e_cpu),
+        "forces_max_abs_diff_vs_cpu": float(np.abs(forces.cpu().numpy() - f_cpu).max()),
+        "cpu_ms": cpu_s * 1e3,
+        "cpu": {"kind": ("reference" if have_ref else "port") + " pair list + numpy forces",
+                "cores": cores if have_ref else 1},
+        "speedup": cpu_s / (gms * 1e-3)}
     return out
 
 

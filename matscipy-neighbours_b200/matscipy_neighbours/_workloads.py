@@ -117,3 +117,24 @@ def diff_lattice(seed=0, shape=(64, 64, 32), spacing=2.8, sigma=0.15,
     return dict(positions=np.ascontiguousarray(pos), cell=cell,
                 pbc=np.array([True, True, True]), cutoff=float(cutoff),
                 quantities="ijdDS")
+
+
+def lj_droplet(n=1_000_000, lattice=1.6, cutoff=2.5, margin=3.0):
+    """The LJ droplet of the reference's molecular-dynamics benchmark (reduced
+    units): the n FCC sites (lattice constant `lattice`) closest to the
+    centroid of an FCC block, centred at the origin, in an open (non-periodic)
+    cubic box that encloses them with `margin` to spare; scalar cutoff."""
+    nc = int(np.ceil(np.cbrt(3.0 * n / (16.0 * np.pi)))) + 2
+    r = np.arange(-nc, nc + 1, dtype=float)
+    g = np.stack(np.meshgrid(r, r, r, indexing="ij"), axis=-1).reshape(-1, 3)
+    basis = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    sites = ((g[:, None, :] + basis[None, :, :]) * lattice).reshape(-1, 3)
+    sites -= sites.mean(axis=0)
+    r2 = np.einsum("ij,ij->i", sites, sites)
+    keep = np.argsort(r2, kind="stable")[:n]
+    pos = np.ascontiguousarray(sites[keep])
+    lo = pos.min(axis=0) - margin
+    hi = pos.max(axis=0) + margin
+    side = float((hi - lo).max())
+    return dict(positions=pos - lo, cell=np.diag([side, side, side]),
+                pbc=np.array([False, False, False]), cutoff=float(cutoff), quantities="ij")
