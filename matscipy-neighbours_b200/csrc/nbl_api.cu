@@ -199,6 +199,24 @@ static int64_t visit_entries(const Batch &b) {
     return n <= kVisitCap ? n : 0;
 }
 
+// Mask-pool words: per system, atoms x (chunks of a full candidate list +
+// one partial chunk per segment batch), with the candidates of an atom
+// estimated as visited cells x atoms per cell; or the demand of the last
+// count on this plan if that was larger.  Items that do not fit are
+// recomputed by the fill, so this only steers speed.
+static int64_t mask_words(const Plan &p, const Batch &b) {
+    double est = 0.0;
+    for (size_t s2 = 0; s2 < b.sys.size(); s2++) {
+        const SysDev &S = b.sys[s2];
+        const double per_cell = (double)S.nat / (double)std::max<int64_t>(b.ncells[s2], 1);
+        const double nv = (double)S.nvisit;
+        est += (double)S.nat * (std::ceil(nv * per_cell / 32.0) + std::ceil(nv / 32.0));
+    }
+    double w = std::max(1.25 * est, 1.1 * (double)p.mask_hint);
+    w = std::min(std::max(w, (double)(int64_t(1) << 20)), (double)(int64_t(1) << 29));
+    return (int64_t)w;
+}
+
 // Carve the per-call buffers out of the plan's workspace.
 static nbl_status layout_workspace(Plan &p, const Batch &b) {
     const int64_t N = b.natoms;
@@ -233,9 +251,9 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_cnt = L.add(sizeof(int32_t) * (N + 1));
     size_t o_off = L.add(sizeof(int64_t) * (N + 1));
     size_t o_small = L.add(sizeof(int) * 8);  // n_home, err, overflow, mask cursor
-    const int64_t mask_cap = std::max<int64_t>(int64_t(1) << 20, 16 * N);
+    const int64_t mask_cap = mask_words(p, b);
     size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
-    size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1));
+    size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1) * kMaskBatches);
     size_t o_items = L.add(sizeof(int2) * std::max<int64_t>(N, 1));
     size_t o_ljp = L.add(sizeof(double) * (size_t)(std::max<int64_t>(N, 1) + N / 1024 + 64));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
@@ -530,13 +548,16 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     if (sync) {
         NBL_CUDA(cudaMemcpyAsync(p.host_small, B.offsets + N, sizeof(int64_t),
                                  cudaMemcpyDeviceToHost, st), "read pair count");
-        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, B.small, sizeof(int) * 2,
+        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, B.small, sizeof(int) * 6,
                                  cudaMemcpyDeviceToHost, st), "read flags");
         NBL_CUDA(cudaStreamSynchronize(st), "count phase");
         p.stage_in_flight = false;
-        int flags[2];
+        int flags[6];
         std::memcpy(flags, p.host_small + 1, sizeof(flags));
         p.npairs = p.host_small[0];
+        unsigned long long demand = 0;  // mask-pool words the count asked for
+        std::memcpy(&demand, flags + 4, sizeof(demand));
+        p.mask_hint = (int64_t)demand;
         if (flags[1] & kErrRange)
             return set_error(NBL_ERROR_RANGE,
                              "positions must be finite and within 2^29 cells of the box");

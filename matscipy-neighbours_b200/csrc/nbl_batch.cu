@@ -384,8 +384,23 @@ NBL_API nbl_status nbl_batch_setup(nbl_batch *bt, const nbl_batch_request *req,
         if (s != NBL_SUCCESS) return s;
         NBL_CUDA(cudaMemcpyAsync(bt->p.host_small, bt->p.bufs.offsets + N, sizeof(int64_t),
                                  cudaMemcpyDeviceToHost, st), "read pair count");
+        NBL_CUDA(cudaMemcpyAsync(bt->p.host_small + 1, bt->p.bufs.small, sizeof(int) * 6,
+                                 cudaMemcpyDeviceToHost, st), "read mask demand");
         NBL_CUDA(cudaStreamSynchronize(st), "count");
         capacity = bt->p.host_small[0] + bt->p.host_small[0] / 4 + 4096;
+        // More hit words asked for than the estimate held: re-plan the
+        // workspace with the measured demand before the graph is captured.
+        int flags[6];
+        std::memcpy(flags, bt->p.host_small + 1, sizeof(flags));
+        unsigned long long demand = 0;
+        std::memcpy(&demand, flags + 4, sizeof(demand));
+        if ((long long)demand > bt->p.bufs.mask_cap) {
+            bt->p.mask_hint = (int64_t)demand;
+            s = upload_batch(bt->p, b, st);
+            if (s != NBL_SUCCESS) return s;
+            NBL_CUDA(cudaStreamSynchronize(st), "batch upload");
+            bt->p.stage_in_flight = false;
+        }
     }
     bt->capacity = capacity;
     const int q = req->quantities;

@@ -709,7 +709,6 @@ k_count(TraverseArgs a) {
         const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
         const int2 hs = c.hs;
-        const bool one_batch = c.nvisit <= kSeg;
         long long mbase = -1;
 
         {
@@ -741,18 +740,19 @@ k_count(TraverseArgs a) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 const int nchunks_all = (total + 31) >> 5;
-                // One word region per work item: (atoms of the i-tile) x (chunks
-                // of the candidate list).
-                if (vb == 0 && a.mask_pool != nullptr) {
+                // One word region per (work item, segment batch): (atoms of the
+                // i-tile) x (chunks of the batch's candidate list).
+                mbase = -1;
+                if (a.mask_pool != nullptr && vb / kSeg < kMaskBatches) {
                     long long base = -1;
-                    if (lane == 0 && one_batch && nchunks_all <= kWinWords) {
+                    if (lane == 0) {
                         const long long words = (long long)ni * nchunks_all;
                         const unsigned long long b =
                             atomicAdd(a.mask_cursor, (unsigned long long)words);
                         if ((long long)b + words <= a.mask_cap) base = (long long)b;
                     }
                     base = __shfl_sync(full, base, 0);
-                    if (lane == 0) a.home_mask[it] = base;
+                    if (lane == 0) a.home_mask[(long long)it * kMaskBatches + vb / kSeg] = base;
                     mbase = base;
                 }
                 // candidate index of atom si itself at offset 0 is kself0 + si
@@ -1059,9 +1059,6 @@ k_fill(TraverseArgs a) {
         const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
         const int2 hs = c.hs;
-        const bool one_batch = c.nvisit <= kSeg;
-        const long long mbase =
-            (a.mask_pool != nullptr && one_batch) ? a.home_mask[it] : -1ll;
 
         {
             const int ib = item.y;
@@ -1093,6 +1090,10 @@ k_fill(TraverseArgs a) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 const int nchunks = (total + 31) >> 5;
+                const long long mbase =
+                    (a.mask_pool != nullptr && vb / kSeg < kMaskBatches)
+                        ? a.home_mask[(long long)it * kMaskBatches + vb / kSeg]
+                        : -1ll;
                 // segment of each tabled candidate: lane = segment
                 if (lane < nseg) {
                     const int e = min(sm.sg.pref[lane + 1], kCandTab);

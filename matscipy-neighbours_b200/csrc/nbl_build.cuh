@@ -75,13 +75,14 @@ struct TraverseArgs {
     // row (global atom index) a, slot s < mat_k of mat_idx / mat_dist instead
     // of the pair list, and mat_count[a] = row length.
     // Hit-mask pool: the count pass stores one 32-bit word per (atom,
-    // 32-candidate chunk) for each home cell it can fit (home_mask[h] = first
-    // word, -1 if none); the fill pass then reads the words instead of
-    // repeating the distance sweep.  mask_pool == nullptr disables it.
+    // 32-candidate chunk) for each (work item, segment batch) it can fit
+    // (home_mask[item * kMaskBatches + batch] = first word, -1 if none); the
+    // fill pass then reads the words instead of repeating the distance
+    // sweep.  mask_pool == nullptr disables it.
     uint32_t *mask_pool;
     unsigned long long *mask_cursor;
     long long mask_cap;
-    long long *home_mask;     // per work item
+    long long *home_mask;     // per (work item, segment batch < kMaskBatches)
     int32_t mat_k;
     int32_t *mat_idx;
     double *mat_dist;
@@ -103,6 +104,12 @@ struct TraverseArgs {
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
+// Segment batches per work item with hit words in the mask pool (a batch is
+// up to 32 visited cells: 27 for the usual 3x3x3 stencil, up to 125 for
+// boxes smaller than the cutoff); home_mask holds kMaskBatches entries per
+// work item.
+constexpr int kMaskBatches = 4;
+
 // Warps per CTA of the pair passes (sizes per-warp partial arrays).
 constexpr int kTraverseWarps = 4;
 

@@ -84,6 +84,7 @@ struct Plan {
     int count_mult = 8;
     int fill_mult = 8;
     int count_group = 4;
+    int64_t mask_hint = 0;    // mask-pool words the last count asked for
     // Row range of nbl_set_atom_range (global atom indices, [lo, hi)).
     int64_t i_lo = 0;
     int64_t i_hi = INT64_MAX;
