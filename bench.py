@@ -408,6 +408,45 @@ def configs_bench(dev, flush, reps=10):
                 "cpu": {"kind": "reference" if have_ref else "port", "cores": 1}}
         out[name] = row
 
+    # List reuse across steps (VerletList) on the dense bulk workload: the
+    # rebuild (cutoff + skin) against a refresh after a small displacement,
+    # both through update() (its host synchronisations included).
+    from matscipy_neighbours.verlet import VerletList
+    wv = W.fcc_bulk(seed=0)
+    posv = torch.from_numpy(wv["positions"]).to(dev)
+    skin = 0.5
+    vl = VerletList(cutoff=wv["cutoff"], skin=skin, cell=wv["cell"], pbc=wv["pbc"])
+    gen = torch.Generator(device=dev).manual_seed(0)
+    kick = 0.01 * torch.randn(posv.shape, dtype=torch.float64, device=dev, generator=gen)
+    bms, rms = [], []
+    for k in range(reps + 3):
+        vl._stored = None  # force a rebuild
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = vl.update(posv)
+        e1.record(stream)
+        del res
+        flush.zero_()
+        e1b = torch.cuda.Event(enable_timing=True)
+        e1b.record(stream)
+        res = vl.update(posv + kick)
+        e2.record(stream)
+        e2.synchronize()
+        del res
+        if k >= 3:
+            bms.append(e0.elapsed_time(e1))
+            rms.append(e1b.elapsed_time(e2))
+    out["verlet_C2"] = {"natoms": int(posv.shape[0]), "cutoff": wv["cutoff"], "skin": skin,
+                        "stored_pairs": int(vl._stored[0].shape[0]),
+                        "rebuild_ms": statistics.median(bms),
+                        "refresh_ms": statistics.median(rms),
+                        "refreshes": vl.refreshes, "builds": vl.builds}
+    del vl, posv, kick
+
     # The fused consumer on the reference's molecular-dynamics benchmark
     # system: LJ forces and energy of a 1,000,000-atom FCC droplet (reduced
     # units, lattice 1.6, cutoff 2.5, open box) with no pair list written

@@ -309,6 +309,29 @@ NBL_API nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double 
                                  double sigma, double *forces, double *energy,
                                  void *stream);
 
+/* ---- list reuse across steps (Verlet list) ------------------------------- */
+
+/* *out (device, one double) = max over the n atoms of |positions - reference|
+   (device, n x 3 each), for the skin test of a reused list.  Asynchronous.
+   No reference counterpart: the reference's MD example rebuilds its list
+   every step (examples/lj_langevin/lj_langevin_gpu.cu:171-179). */
+NBL_API nbl_status nbl_max_displacement(int64_t n, const double *positions,
+                                        const double *reference, double *out, void *stream);
+
+/* Refreshes a stored list (first, second, shift: device, built with a larger
+   cutoff) at the current device positions: D = r_j - r_i + sum over periodic
+   axes of S_m cell[m] (cell: host row-major 3x3, rows are lattice vectors;
+   pbc: host[3]), d = |D|, and keeps the pairs with d < cutoff, in the stored
+   order, into `out` (device; NULL members are skipped).  Sets *nkept
+   (synchronises `stream`); NBL_ERROR_CAPACITY if `capacity` is too small;
+   out == NULL only counts.  No reference counterpart (see above). */
+NBL_API nbl_status nbl_verlet_refresh(int64_t npairs, const int32_t *first,
+                                      const int32_t *second, const int32_t *shift,
+                                      const double *positions, const double *cell,
+                                      const uint8_t *pbc, double cutoff,
+                                      const nbl_outputs *out, int64_t capacity,
+                                      int64_t *nkept, void *stream);
+
 /* ---- CSR helpers of a pair list, on the device --------------------------- */
 
 /* Row starts of an i-sorted pair list (all pointers device memory):
