@@ -229,7 +229,7 @@ def batched_bench(steps, warmup, dev, rank=0):
             "speedup": plain_s / batched_s}
 
 
-def configs_bench(dev, flush, reps=10):
+def configs_bench(dev, flush, reps=10, only=None):
     """The other configurations beside the headline (rank 0, N = 1): C1 plain
     small, C3 sparse slab (per-type cutoffs, ijdD), C5 differentiation lattice.
     Each: positions resident on the device, median of `reps` full builds
@@ -258,9 +258,15 @@ def configs_bench(dev, flush, reps=10):
     sptr = ctypes.c_void_p(stream.cuda_stream)
     plan = ext.plan_for(dev.index)
     out = {}
-    for name, w in (("C1_plain_small", W.plain_small()),
-                    ("C3_sparse_slab", W.sparse_slab()),
-                    ("C5_diff_lattice", W.diff_lattice())):
+    def wanted(name):
+        return only is None or name in only
+
+    for name, make in (("C1_plain_small", W.plain_small),
+                       ("C3_sparse_slab", W.sparse_slab),
+                       ("C5_diff_lattice", W.diff_lattice)):
+        if not wanted(name):
+            continue
+        w = make()
         q = w["quantities"]
         flags = ext.quantity_flags(q)
         nat = w["positions"].shape[0]
@@ -408,9 +414,18 @@ def configs_bench(dev, flush, reps=10):
                 "cpu": {"kind": "reference" if have_ref else "port", "cores": 1}}
         out[name] = row
 
-    # List reuse across steps (VerletList) on the dense bulk workload: the
-    # rebuild (cutoff + skin) against a refresh after a small displacement,
-    # both through update() (its host synchronisations included).
+    if wanted("verlet_C2"):
+        _verlet_line(out, dev, flush, reps, stream, W)
+    if wanted("LJ_droplet_1M"):
+        _lj_line(out, dev, flush, reps, stream, sptr, plan, W, O, ext, have_ref, cpu_fn, cores)
+    return out
+
+
+def _verlet_line(out, dev, flush, reps, stream, W):
+    """List reuse across steps (VerletList) on the dense bulk workload: the
+    rebuild (cutoff + skin) against a refresh after a small displacement,
+    both through update() (its host synchronisations included)."""
+    import torch
     from matscipy_neighbours.verlet import VerletList
     wv = W.fcc_bulk(seed=0)
     posv = torch.from_numpy(wv["positions"]).to(dev)
@@ -447,11 +462,17 @@ def configs_bench(dev, flush, reps=10):
                         "refreshes": vl.refreshes, "builds": vl.builds}
     del vl, posv, kick
 
-    # The fused consumer on the reference's molecular-dynamics benchmark
-    # system: LJ forces and energy of a 1,000,000-atom FCC droplet (reduced
-    # units, lattice 1.6, cutoff 2.5, open box) with no pair list written
-    # (nbl_lj_forces), against the reference's CPU core building the pair
-    # list (all host threads) plus float64 numpy force sums.
+
+def _lj_line(out, dev, flush, reps, stream, sptr, plan, W, O, ext, have_ref, cpu_fn, cores):
+    """The fused consumer on the reference's molecular-dynamics benchmark
+    system: LJ forces and energy of a 1,000,000-atom FCC droplet (reduced
+    units, lattice 1.6, cutoff 2.5, open box) with no pair list written
+    (nbl_lj_forces), against the reference's CPU core building the pair list
+    (all host threads) plus float64 numpy force sums."""
+    import ctypes
+
+    import numpy as np
+    import torch
     w = W.lj_droplet()
     nat = w["positions"].shape[0]
     cell = np.ascontiguousarray(w["cell"], dtype=float)
@@ -501,7 +522,6 @@ def configs_bench(dev, flush, reps=10):
         "cpu": {"kind": ("reference" if have_ref else "port") + " pair list + numpy forces",
                 "cores": cores if have_ref else 1},
         "speedup": cpu_s / (gms * 1e-3)}
-    return out
 
 
 def cpu_baseline(steps=2):
@@ -584,6 +604,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the C1/C3/C5 lines (and the backward timing)")
+    ap.add_argument("--only-configs", default=None,
+                    help="comma-separated config lines to run alone (e.g. C5_diff_lattice, "
+                         "LJ_droplet_1M, verlet_C2); prints them and nothing else")
     ap.add_argument("--reps", type=int, default=64,
                     help="FCC unit cells per edge (64 = the benchmark size; smaller "
                          "values make the small cases used for profiling)")
@@ -608,6 +631,11 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.only_configs:
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        only = set(x.strip() for x in args.only_configs.split(",") if x.strip())
+        print(json.dumps({"configs": configs_bench(dev, flush, only=only)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
