@@ -143,6 +143,15 @@ NBL_API nbl_status nbl_plan_trim(nbl_plan *plan);
    (src/libneighbours/neighbour_list.cc:99-204). */
 NBL_API nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi);
 
+/* Launch configuration of the plan's pair passes: CTAs per SM of the count
+   and fill grids (0: two full waves of the kernel's resident CTAs, the
+   default) and atoms per sweep in the FP32 count (2 or 4; 0 keeps 4).  Takes
+   effect at the next nbl_count.  A tuning knob with no effect on results.  No
+   reference counterpart (the reference's core is serial per cell,
+   src/libneighbours/neighbour_list.cc:99-204). */
+NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, int count_group,
+                                       int fill_ctas_per_sm);
+
 /* Count phase: bins the atoms, counts every atom's neighbours and scans the
    counts into row offsets.  Host positions are copied in on `stream`.
    Synchronises `stream` to return the pair count. */

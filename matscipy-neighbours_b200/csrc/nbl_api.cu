@@ -356,9 +356,15 @@ nbl_status finish_batch(Batch &b, int grid_req) {
 // count / fill
 // ---------------------------------------------------------------------------
 
-static int traverse_grid(const Plan &p, int64_t natoms, int mult) {
-    // Persistent-style grid: a few resident CTAs per SM (four warps each, one
-    // work item per warp at a time), capped by the number of work items.
+// Persistent-style grid: `mult` CTAs per SM (four warps each, one work item
+// per warp at a time; mult <= 0: kAutoWaves full waves of the kernel's
+// resident CTAs), capped by the number of work items.  The warps take work
+// items in a fixed stride, so a grid that is not a whole number of waves
+// leaves its last partial wave running alone.
+static int traverse_grid(const Plan &p, int64_t natoms, int mult, int mode, bool fp32,
+                         int kind, int group, bool lj) {
+    if (mult <= 0)
+        mult = kAutoWaves * std::max(1, traverse_blocks_per_sm(mode, fp32, kind, group, lj));
     const int64_t items = std::max<int64_t>((natoms + 3) / 4, 1);
     return (int)std::min<int64_t>((int64_t)p.num_sms * mult, items);
 }
@@ -528,9 +534,10 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.i_hi = p.i_hi;
     if (p.i_lo > 0 || p.i_hi < N)
         NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
-    p.trav_grid = traverse_grid(p, N, p.count_mult);
-    p.fill_grid = traverse_grid(p, N, p.fill_mult);
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
+    p.trav_grid = traverse_grid(p, N, p.count_mult, kModeCount, b.fp32, p.batch_kind,
+                                p.count_group, false);
+    p.fill_grid = traverse_grid(p, N, p.fill_mult, kModeFill, b.fp32, p.batch_kind, 4, false);
     NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
                              p.count_group),
              "count pass");
@@ -754,6 +761,20 @@ nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi) {
     return NBL_SUCCESS;
 }
 
+nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, int count_group,
+                               int fill_ctas_per_sm) {
+    clear_error();
+    if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan");
+    if (count_ctas_per_sm < 0 || count_ctas_per_sm > 64 || fill_ctas_per_sm < 0 ||
+        fill_ctas_per_sm > 64 || !(count_group == 0 || count_group == 2 || count_group == 4))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT,
+                         "launch: CTAs per SM in [0, 64], count group 0, 2 or 4");
+    plan->p.count_mult = count_ctas_per_sm;
+    plan->p.fill_mult = fill_ctas_per_sm;
+    plan->p.count_group = count_group == 0 ? 4 : count_group;
+    return NBL_SUCCESS;
+}
+
 nbl_status nbl_count(nbl_plan *plan, const nbl_request *req, void *stream,
                      int64_t *npairs) {
     clear_error();
@@ -898,7 +919,9 @@ nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
     ta.lj_eps4 = 4.0 * epsilon;
     ta.lj_eps24 = 24.0 * epsilon;
     ta.lj_sig2 = sigma * sigma;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, cs),
+    const int grid = traverse_grid(p, b.natoms, p.fill_mult, kModeFill, p.batch_fp32,
+                                   p.batch_kind, 4, true);
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, grid, cs),
              "force pass");
     NBL_CUDA(launch_lj_energy(p.bufs.lj_part, b.natoms, p.bufs.lj_part + b.natoms, energy,
                               cs),

@@ -235,7 +235,7 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         max_visit = std::max(max_visit, b.sys[s].nvisit);
     }
     char key[160];
-    std::snprintf(key, sizeof(key), "sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
+    std::snprintf(key, sizeof(key), "w2_sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
                   b.sys.empty() ? 0 : b.sys[0].cutoff_kind, b.fp32 ? 1 : 0,
                   bucket_log2(b.natoms / std::max(cells, 1.0)), bucket_log2(max_visit));
     bt->tune_key = key;
@@ -255,11 +255,15 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
     NBL_CUDA(cudaEventCreate(&e1), "event");
     TuneChoice best{bt->p.count_mult, bt->p.count_group, bt->p.fill_mult};
     float best_ms = 1e30f;
-    const int mults[] = {4, 8, 16};
+    // grids of 1, 2 and 4 full waves of each kernel's resident CTAs
+    const int waves[] = {1, 2, 4};
     const int groups[] = {2, 4};
+    const int kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
     for (int g : groups) {
         if (!b.fp32 && g != 4) continue;  // the group only shapes the FP32 sweep
-        for (int m : mults) {
+        const int occ = std::max(1, traverse_blocks_per_sm(kModeCount, b.fp32, kind, g));
+        for (int wv : waves) {
+            const int m = wv * occ;
             bt->p.count_mult = m;
             bt->p.count_group = g;
             const float ms = time_count(bt, st, e0, e1);
@@ -277,12 +281,20 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         cudaEventDestroy(e1);
         return NBL_ERROR_INTERNAL;
     }
+    bt->p.have_count = true;  // the fill below reads this count's offsets
     best_ms = 1e30f;
-    for (int m : mults) {
+    const int focc = std::max(1, traverse_blocks_per_sm(kModeFill, b.fp32, kind));
+    for (int wv : waves) {
+        const int m = wv * focc;
         bt->p.fill_mult = m;
         bt->p.fill_grid = std::max(1, std::min(bt->p.num_sms * m, (int)std::max<int64_t>(
                                                                     (b.natoms + 3) / 4, 1)));
         const float ms = time_fill(bt, st, e0, e1);
+        if (ms >= 1e30f) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return NBL_ERROR_INTERNAL;
+        }
         if (ms < best_ms) {
             best_ms = ms;
             best.fill_mult = m;

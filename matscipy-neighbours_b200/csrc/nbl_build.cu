@@ -26,6 +26,7 @@
 // drained 32 pairs at a time so that the FP64 epilogue and the stores run
 // with full warps and near-contiguous addresses.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <type_traits>
@@ -339,24 +340,34 @@ struct __align__(16) CountSmem {
 };
 
 constexpr int kCandTab = 1024;   // candidates with a segment-table entry (fill)
-constexpr int kPosTab = 704;     // pairs per window with a position table (fill)
+constexpr int kPosTab = 640;     // pairs per window with a position table (fill)
 static_assert(kRange <= 8192 && kITile <= 32,
               "position-table entries hold the candidate in 13 bits, the atom in 5");
 
+// Per-warp fill state, about 9.3 KB, so that six 4-warp CTAs fit an SM
+// (the force sink's sums live in a separate array of the force-sink kernel).
 template <bool FP32>
 struct __align__(16) FillSmem {
     SegSmem sg;
-    CandT<FP32> cand[FillTile<FP32>::kCand];
     double4 i64[kITile];
-    float4 i32[kITile];
     int4 iaux[kITile];
     int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     long long icur[kITile];
-    double facc[kITile][4];    // force sink: the tile's force and energy sums
     uint32_t mw[kWinWords];
     int32_t mpre[kWinWords + 1];
-    uint32_t ptab[kPosTab];    // window position -> candidate | atom << 13 (small windows)
+    union {
+        uint32_t ptab[kPosTab];  // window position -> candidate | atom << 13 (small windows)
+        CandT<FP32> cand[FillTile<FP32>::kCand];  // staged candidates (recomputed words)
+    };
     uint8_t cand_seg[kCandTab];     // segment of each of the batch's first candidates
+};
+static_assert(4 * sizeof(FillSmem<true>) <= 37888 && 4 * sizeof(FillSmem<false>) <= 37888,
+              "six fill CTAs per SM: at most 37 KB of shared memory per CTA");
+
+// Resident CTAs per SM the fill is compiled for (registers and shared memory).
+template <bool LJ>
+struct FillOcc {
+    static constexpr int kBlocks = LJ ? 5 : 5;
 };
 
 // Per-home-cell constants kept in registers.
@@ -997,8 +1008,8 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
 // atom (runs of equal i are contiguous) and the run's last lane adds them to
 // the tile's shared-memory sums.
 template <bool FP32>
-__device__ __forceinline__ void lj_round(FillSmem<FP32> &sm, const TraverseArgs &a,
-                                         const PairWork &w, int lane) {
+__device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc)[4],
+                                         const TraverseArgs &a, const PairWork &w, int lane) {
     const unsigned full = 0xffffffffu;
     double f0 = 0.0, f1 = 0.0, f2 = 0.0, e = 0.0;
     const int il = w.act ? w.il : -1;
@@ -1034,25 +1045,27 @@ __device__ __forceinline__ void lj_round(FillSmem<FP32> &sm, const TraverseArgs 
     }
     const int inext = __shfl_down_sync(full, il, 1);
     if (il >= 0 && (lane == 31 || inext != il)) {
-        sm.facc[il][0] += f0;
-        sm.facc[il][1] += f1;
-        sm.facc[il][2] += f2;
-        sm.facc[il][3] += e;
+        facc[il][0] += f0;
+        facc[il][1] += f1;
+        facc[il][2] += f2;
+        facc[il][3] += e;
     }
     __syncwarp();
 }
 
-template <bool FP32, int KIND>
-__global__ void __launch_bounds__(kThreads, 4)
+template <bool FP32, int KIND, bool LJ>
+__global__ void __launch_bounds__(kThreads, FillOcc<LJ>::kBlocks)
 k_fill(TraverseArgs a) {
     constexpr int kCand = FillTile<FP32>::kCand;
     __shared__ FillSmem<FP32> smem[kWarps];
+    // force sink: each warp's tile force and energy sums
+    __shared__ double facc_all[LJ ? kWarps * kITile : 1][4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FillSmem<FP32> &sm = smem[warp];
+    double(*facc)[4] = facc_all + (LJ ? warp * kITile : 0);
     const unsigned full = 0xffffffffu;
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
-    const bool lj = a.lj_force != nullptr;
 
     for (int it = gwarp; it < nitems; it += nwarps) {
         const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
@@ -1076,12 +1089,11 @@ k_fill(TraverseArgs a) {
                 if (in) {
                     const int c2 = __popc(im & lanemask_lt());
                     const int si = ib + lane;
-                    sm.i32[c2] = a.pos32[si];
                     sm.i64[c2] = a.pos64[si];
                     sm.iaux[c2] = ax;
                     sm.isi[c2] = si;
                     sm.icur[c2] = (long long)a.offsets[ax.x];
-                    sm.facc[c2][0] = sm.facc[c2][1] = sm.facc[c2][2] = sm.facc[c2][3] = 0.0;
+                    if (LJ) facc[c2][0] = facc[c2][1] = facc[c2][2] = facc[c2][3] = 0.0;
                 }
                 __syncwarp();
             }
@@ -1124,7 +1136,7 @@ k_fill(TraverseArgs a) {
                                 stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
                                 for (int al = 0; al < na; al++) {
                                     const int il = a0 + al, si = sm.isi[il];
-                                    const float4 pi32 = sm.i32[il];
+                                    const float4 pi32 = a.pos32[si];
                                     const double4 pi64 = sm.i64[il];
                                     const int kself_tile = kself0 + si - (kr + kt);
                                     for (int ch = 0; ch < (nkp >> 5); ch++) {
@@ -1180,8 +1192,8 @@ k_fill(TraverseArgs a) {
                             const PairWork nxt = fetch_pair<FP32>(sm, a, nseg, nchunks, nw,
                                                                   nch, inv_nch, kr, a0, carry,
                                                                   P0 + 32 + lane, tab);
-                            if (lj)
-                                lj_round<FP32>(sm, a, cur, lane);
+                            if (LJ)
+                                lj_round<FP32>(sm, facc, a, cur, lane);
                             else
                                 store_pair<FP32>(sm, a, H, cur);
                             cur = nxt;
@@ -1203,11 +1215,11 @@ k_fill(TraverseArgs a) {
                     a.mat_count[ax] = (int32_t)deg;
                     if (deg > a.mat_k) atomicOr(a.mat_overflow, 1);
                 }
-                if (lj) {
-                    a.lj_force[3 * (long long)ax + 0] = sm.facc[lane][0];
-                    a.lj_force[3 * (long long)ax + 1] = sm.facc[lane][1];
-                    a.lj_force[3 * (long long)ax + 2] = sm.facc[lane][2];
-                    a.lj_energy[ax] = sm.facc[lane][3];
+                if (LJ) {
+                    a.lj_force[3 * (long long)ax + 0] = facc[lane][0];
+                    a.lj_force[3 * (long long)ax + 1] = facc[lane][1];
+                    a.lj_force[3 * (long long)ax + 2] = facc[lane][2];
+                    a.lj_energy[ax] = facc[lane][3];
                 }
             }
             __syncwarp();
@@ -1218,7 +1230,8 @@ k_fill(TraverseArgs a) {
 #define NBL_INST(F, K)                                            \
     template __global__ void k_count<F, K, 2>(TraverseArgs);      \
     template __global__ void k_count<F, K, 4>(TraverseArgs);      \
-    template __global__ void k_fill<F, K>(TraverseArgs);
+    template __global__ void k_fill<F, K, false>(TraverseArgs);   \
+    template __global__ void k_fill<F, K, true>(TraverseArgs);
 NBL_INST(true, kCutScalar)
 NBL_INST(true, kCutPerAtom)
 NBL_INST(true, kCutPerType)
@@ -1309,6 +1322,56 @@ cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+namespace {
+
+template <typename K>
+int occupancy_of(K kern) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+template <bool F, int K>
+int occupancy_fk(int mode, int group, bool lj) {
+    if (mode == kModeCount) return group == 2 ? occupancy_of(k_count<F, K, 2>)
+                                              : occupancy_of(k_count<F, K, 4>);
+    return lj ? occupancy_of(k_fill<F, K, true>) : occupancy_of(k_fill<F, K, false>);
+}
+
+}  // namespace
+
+int traverse_blocks_per_sm(int mode, bool fp32, int kind, int group, bool lj) {
+    // cached per device and kernel
+    constexpr int kDev = 16;
+    static std::atomic<int> cache[kDev][2][2][3][2][2];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDev) {
+        cudaGetLastError();
+        dev = -1;
+    }
+    const int mi = mode == kModeCount ? 0 : 1, fi = fp32 ? 1 : 0, gi = group == 2 ? 0 : 1;
+    const int ki = kind == kCutPerAtom ? 1 : (kind == kCutPerType ? 2 : 0), li = lj ? 1 : 0;
+    if (dev >= 0) {
+        const int c = cache[dev][mi][fi][ki][gi][li].load(std::memory_order_relaxed);
+        if (c > 0) return c;
+    }
+    int n = 0;
+    if (fp32) {
+        n = ki == 1 ? occupancy_fk<true, kCutPerAtom>(mode, group, lj)
+                    : (ki == 2 ? occupancy_fk<true, kCutPerType>(mode, group, lj)
+                               : occupancy_fk<true, kCutScalar>(mode, group, lj));
+    } else {
+        n = ki == 1 ? occupancy_fk<false, kCutPerAtom>(mode, group, lj)
+                    : (ki == 2 ? occupancy_fk<false, kCutPerType>(mode, group, lj)
+                               : occupancy_fk<false, kCutScalar>(mode, group, lj));
+    }
+    if (dev >= 0 && n > 0) cache[dev][mi][fi][ki][gi][li].store(n, std::memory_order_relaxed);
+    return n;
+}
+
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, int group) {
     if (grid <= 0) return cudaSuccess;
@@ -1319,7 +1382,13 @@ cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a
         else                                                               \
             k_count<F, K, 4><<<grid, kThreads, 0, st>>>(a);                \
     } while (0)
-#define NBL_GO_F(F, K) k_fill<F, K><<<grid, kThreads, 0, st>>>(a)
+#define NBL_GO_F(F, K)                                                     \
+    do {                                                                   \
+        if (a.lj_force != nullptr)                                         \
+            k_fill<F, K, true><<<grid, kThreads, 0, st>>>(a);              \
+        else                                                               \
+            k_fill<F, K, false><<<grid, kThreads, 0, st>>>(a);             \
+    } while (0)
 #define NBL_BY_KIND(GO, F)                            \
     do {                                              \
         if (kind == kCutPerAtom)                      \

@@ -126,5 +126,9 @@ cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *ta
 // group: atoms swept together per pass in the FP32 count (2 or 4).
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, int group = 4);
+// CTAs of the pair pass (mode, precision, cutoff kind, count group, force
+// sink) resident per SM on the current device: the grid of one full wave is
+// this times the SM count.  0 on error.
+int traverse_blocks_per_sm(int mode, bool fp32, int kind, int group = 4, bool lj = false);
 
 }  // namespace nbl

@@ -71,6 +71,9 @@ struct Workspace {
     void release();
 };
 
+// Full waves of resident CTAs in the default grid of a pair pass.
+constexpr int kAutoWaves = 2;
+
 struct Plan {
     int device = 0;
     int num_sms = 148;
@@ -79,10 +82,11 @@ struct Plan {
     TraverseArgs targs{};
     int trav_grid = 0;        // count-pass grid (CTAs)
     int fill_grid = 0;        // fill-pass grid (CTAs)
-    // Launch configuration (set by the autotuner for batches): CTAs per SM
-    // of the count and fill passes, atoms per sweep pass in the count.
-    int count_mult = 8;
-    int fill_mult = 8;
+    // Launch configuration (set by the autotuner for batches, or by
+    // nbl_plan_set_launch): CTAs per SM of the count and fill passes (0: a
+    // whole number of waves of resident CTAs), atoms per sweep in the count.
+    int count_mult = 0;
+    int fill_mult = 0;
     int count_group = 4;
     int64_t mask_hint = 0;    // mask-pool words the last count asked for
     // Row range of nbl_set_atom_range (global atom indices, [lo, hi)).

@@ -81,6 +81,7 @@ def _load():
         "nbl_plan_destroy": ([P], ctypes.c_int),
         "nbl_plan_trim": ([P], ctypes.c_int),
         "nbl_set_atom_range": ([P, ctypes.c_int64, ctypes.c_int64], ctypes.c_int),
+        "nbl_plan_set_launch": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "nbl_count": ([P, ctypes.POINTER(Request), P, ctypes.POINTER(ctypes.c_int64)],
                       ctypes.c_int),
         "nbl_fill": ([P, ctypes.POINTER(Outputs), P], ctypes.c_int),

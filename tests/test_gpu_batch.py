@@ -99,7 +99,8 @@ def test_batch_autotune_picks_a_config(oracle):
     systems = _systems(nsys=24, seed=4)
     b = NeighbourListBatch(systems, autotune=True)
     cm, grp, fm = b.config()
-    assert cm in (4, 8, 16) and grp in (2, 4) and fm in (4, 8, 16)
+    # CTAs per SM: 1, 2 or 4 waves of each kernel's resident CTAs
+    assert 1 <= cm <= 64 and grp in (2, 4) and 1 <= fm <= 64
     b.run()
     _check(oracle, b, systems)
     b.close()
