@@ -333,7 +333,9 @@ NBL_API nbl_status nbl_max_displacement(int64_t n, const double *positions,
    pbc: host[3]), d = |D|, and keeps the pairs with d < cutoff, in the stored
    order, into `out` (device; NULL members are skipped).  Sets *nkept
    (synchronises `stream`); NBL_ERROR_CAPACITY if `capacity` is too small;
-   out == NULL only counts.  No reference counterpart (see above). */
+   out == NULL only counts.  With capacity >= npairs the pairs are written
+   before the one synchronisation (a single call per step).  No reference
+   counterpart (see above). */
 NBL_API nbl_status nbl_verlet_refresh(int64_t npairs, const int32_t *first,
                                       const int32_t *second, const int32_t *shift,
                                       const double *positions, const double *cell,

@@ -95,39 +95,90 @@ __device__ __forceinline__ void pair_d(const Cell &C, const double *r, int32_t i
          (s0 * C.c[2] + s1 * C.c[5] + s2 * C.c[8]);
 }
 
-__global__ void k_refresh_flag(Cell C, const int32_t *__restrict__ fi,
-                               const int32_t *__restrict__ fj, const int32_t *__restrict__ fS,
-                               const double *__restrict__ r, int64_t np, double rc2,
-                               int32_t *__restrict__ keep) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    double dx, dy, dz;
+// Refresh in two passes over the stored pairs, kRTile pairs per block in
+// kRTile / kRThreads sub-tiles of one pair per thread: the first counts the
+// kept pairs of each block, the second (after a scan of the block counts)
+// recomputes the test and writes the kept pairs at the block's offset plus
+// their rank inside the block, so the stored order is kept.
+constexpr int kRThreads = 256;
+constexpr int kRTile = 2048;
+constexpr int kRWarps = kRThreads / 32;
+
+__device__ __forceinline__ bool refresh_keep(const Cell &C, const int32_t *__restrict__ fi,
+                                             const int32_t *__restrict__ fj,
+                                             const int32_t *__restrict__ fS,
+                                             const double *__restrict__ r, int64_t p,
+                                             int64_t np, double rc2, double &dx, double &dy,
+                                             double &dz) {
+    if (p >= np) return false;
     pair_d(C, r, fi[p], fj[p], fS + 3 * p, dx, dy, dz);
-    keep[p] = (dx * dx + dy * dy + dz * dz) < rc2 ? 1 : 0;
+    return (dx * dx + dy * dy + dz * dz) < rc2;
 }
 
-__global__ void k_refresh_scatter(Cell C, const int32_t *__restrict__ fi,
-                                  const int32_t *__restrict__ fj,
-                                  const int32_t *__restrict__ fS, const double *__restrict__ r,
-                                  int64_t np, const int32_t *__restrict__ keep,
-                                  const int64_t *__restrict__ pos, nbl_outputs o) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np || !keep[p]) return;
-    const int64_t q = pos[p];
-    double dx, dy, dz;
-    pair_d(C, r, fi[p], fj[p], fS + 3 * p, dx, dy, dz);
-    if (o.first) o.first[q] = fi[p];
-    if (o.second) o.second[q] = fj[p];
-    if (o.distvec) {
-        o.distvec[3 * q] = dx;
-        o.distvec[3 * q + 1] = dy;
-        o.distvec[3 * q + 2] = dz;
+__global__ void __launch_bounds__(kRThreads)
+k_refresh_count(Cell C, const int32_t *__restrict__ fi, const int32_t *__restrict__ fj,
+                const int32_t *__restrict__ fS, const double *__restrict__ r, int64_t np,
+                double rc2, int32_t *__restrict__ blk) {
+    __shared__ int wsum[kRWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p0 = (int64_t)blockIdx.x * kRTile;
+    int c = 0;
+#pragma unroll 2
+    for (int k = 0; k < kRTile / kRThreads; k++) {
+        double dx, dy, dz;
+        const bool keep = refresh_keep(C, fi, fj, fS, r, p0 + k * kRThreads + threadIdx.x, np,
+                                       rc2, dx, dy, dz);
+        c += __popc(__ballot_sync(0xffffffffu, keep));
     }
-    if (o.absdist) o.absdist[q] = sqrt(dx * dx + dy * dy + dz * dz);
-    if (o.shift) {
-        o.shift[3 * q] = fS[3 * p];
-        o.shift[3 * q + 1] = fS[3 * p + 1];
-        o.shift[3 * q + 2] = fS[3 * p + 2];
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kRWarps; w++) t += wsum[w];
+        blk[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kRThreads)
+k_refresh_write(Cell C, const int32_t *__restrict__ fi, const int32_t *__restrict__ fj,
+                const int32_t *__restrict__ fS, const double *__restrict__ r, int64_t np,
+                double rc2, const int64_t *__restrict__ blk_off, nbl_outputs o) {
+    __shared__ int wcnt[kRWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p0 = (int64_t)blockIdx.x * kRTile;
+    int64_t base = blk_off[blockIdx.x];
+    for (int k = 0; k < kRTile / kRThreads; k++) {
+        const int64_t p = p0 + k * kRThreads + threadIdx.x;
+        double dx, dy, dz;
+        const bool keep = refresh_keep(C, fi, fj, fS, r, p, np, rc2, dx, dy, dz);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) wcnt[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kRWarps; w++) {
+            const int x = wcnt[w];
+            before += (w < warp) ? x : 0;
+            total += x;
+        }
+        __syncthreads();  // wcnt is rewritten by the next sub-tile
+        if (keep) {
+            const int64_t q = base + before + __popc(m & ((1u << lane) - 1u));
+            if (o.first) o.first[q] = fi[p];
+            if (o.second) o.second[q] = fj[p];
+            if (o.distvec) {
+                o.distvec[3 * q] = dx;
+                o.distvec[3 * q + 1] = dy;
+                o.distvec[3 * q + 2] = dz;
+            }
+            if (o.absdist) o.absdist[q] = sqrt(dx * dx + dy * dy + dz * dz);
+            if (o.shift) {
+                o.shift[3 * q] = fS[3 * p];
+                o.shift[3 * q + 1] = fS[3 * p + 1];
+                o.shift[3 * q + 2] = fS[3 * p + 2];
+            }
+        }
+        base += total;
     }
 }
 
@@ -195,6 +246,8 @@ extern "C" NBL_API nbl_status nbl_verlet_refresh(int64_t npairs, const int32_t *
     Cell C;
     std::memcpy(C.c, cell, sizeof(C.c));
     C.pbc_bits = (pbc[0] ? 1 : 0) | (pbc[1] ? 2 : 0) | (pbc[2] ? 4 : 0);
+    const double rc2 = cutoff * cutoff;
+    const int64_t nblk = (npairs + kRTile - 1) / kRTile;
     char *scratch = nullptr;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -204,38 +257,46 @@ extern "C" NBL_API nbl_status nbl_verlet_refresh(int64_t npairs, const int32_t *
         bytes += (b + 255) & ~size_t(255);
         return o;
     };
-    const size_t o_keep = add(sizeof(int32_t) * npairs);
-    const size_t o_pos = add(sizeof(int64_t) * (npairs + 1));
-    const size_t o_s = add(sizeof(int64_t) * scan_scratch_elems(npairs + 1));
-    const unsigned grid = (unsigned)((npairs + 255) / 256);
+    const size_t o_blk = add(sizeof(int32_t) * nblk);
+    const size_t o_off = add(sizeof(int64_t) * (nblk + 1));
+    const size_t o_s = add(sizeof(int64_t) * scan_scratch_elems(nblk + 1));
+    // With room for every stored pair the write pass needs no count first:
+    // one synchronisation at the end reads the total.
+    const bool direct = out != nullptr && capacity >= npairs;
     {
         cudaMemPool_t pool = nullptr;
         V_CUDA(scratch_pool(dev, &pool), "scratch pool");
         V_CUDA(cudaMallocFromPoolAsync((void **)&scratch, bytes, pool, st), "scratch");
-        int32_t *keep = reinterpret_cast<int32_t *>(scratch + o_keep);
-        int64_t *pos = reinterpret_cast<int64_t *>(scratch + o_pos);
+        int32_t *blk = reinterpret_cast<int32_t *>(scratch + o_blk);
+        int64_t *off = reinterpret_cast<int64_t *>(scratch + o_off);
         int64_t *sscr = reinterpret_cast<int64_t *>(scratch + o_s);
-        k_refresh_flag<<<grid, 256, 0, st>>>(C, first, second, shift, positions, npairs,
-                                             cutoff * cutoff, keep);
+        k_refresh_count<<<(unsigned)nblk, kRThreads, 0, st>>>(C, first, second, shift, positions,
+                                                              npairs, rc2, blk);
         count_launch();
-        V_CUDA(cudaGetLastError(), "refresh flags");
-        V_CUDA(exclusive_scan_i32_i64(keep, npairs, pos, sscr, st), "scan");
+        V_CUDA(cudaGetLastError(), "refresh count");
+        V_CUDA(exclusive_scan_i32_i64(blk, nblk, off, sscr, st), "scan");
+        if (direct) {
+            k_refresh_write<<<(unsigned)nblk, kRThreads, 0, st>>>(C, first, second, shift,
+                                                                  positions, npairs, rc2, off,
+                                                                  *out);
+            count_launch();
+            V_CUDA(cudaGetLastError(), "refresh write");
+        }
         int64_t total = 0;  // pageable: the copy completes before it returns
-        V_CUDA(cudaMemcpyAsync(&total, pos + npairs, sizeof(int64_t), cudaMemcpyDeviceToHost,
-                               st),
+        V_CUDA(cudaMemcpyAsync(&total, off + nblk, sizeof(int64_t), cudaMemcpyDeviceToHost, st),
                "read count");
         V_CUDA(cudaStreamSynchronize(st), "refresh count");
         *nkept = total;
-        if (!out || total == 0) goto done;
+        if (!out || direct || total == 0) goto done;
         if (capacity < total) {
             status = set_error(NBL_ERROR_CAPACITY, "verlet_refresh: %lld pairs, capacity %lld",
                                (long long)total, (long long)capacity);
             goto done;
         }
-        k_refresh_scatter<<<grid, 256, 0, st>>>(C, first, second, shift, positions, npairs,
-                                                keep, pos, *out);
+        k_refresh_write<<<(unsigned)nblk, kRThreads, 0, st>>>(C, first, second, shift, positions,
+                                                              npairs, rc2, off, *out);
         count_launch();
-        V_CUDA(cudaGetLastError(), "refresh scatter");
+        V_CUDA(cudaGetLastError(), "refresh write");
     }
 done:
     if (scratch) cudaFreeAsync(scratch, st);

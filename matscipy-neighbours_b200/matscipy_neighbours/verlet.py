@@ -103,30 +103,30 @@ class VerletList:
         stream = torch.cuda.current_stream(pos.device)
         sp = ctypes.c_void_p(stream.cuda_stream)
         n = ctypes.c_int64()
-        args = (np_, ctypes.c_void_p(i.data_ptr()) if np_ else None,
+        dev = pos.device
+        # room for every stored pair: one call writes the kept ones and
+        # returns their number; the results are views of the first n rows
+        want = set(self.quantities)
+        bufs = {"i": torch.empty(np_ if "i" in want else 0, dtype=torch.int32, device=dev),
+                "j": torch.empty(np_ if "j" in want else 0, dtype=torch.int32, device=dev),
+                "D": torch.empty((np_ if "D" in want else 0, 3), dtype=torch.float64, device=dev),
+                "d": torch.empty(np_ if "d" in want else 0, dtype=torch.float64, device=dev),
+                "S": torch.empty((np_ if "S" in want else 0, 3), dtype=torch.int32, device=dev)}
+        o = _ext.Outputs()
+        o.first = bufs["i"].data_ptr() if "i" in want and np_ else None
+        o.second = bufs["j"].data_ptr() if "j" in want and np_ else None
+        o.distvec = bufs["D"].data_ptr() if "D" in want and np_ else None
+        o.absdist = bufs["d"].data_ptr() if "d" in want and np_ else None
+        o.shift = bufs["S"].data_ptr() if "S" in want and np_ else None
+        with torch.cuda.device(dev):
+            _ext.check(self._lib.nbl_verlet_refresh(
+                np_, ctypes.c_void_p(i.data_ptr()) if np_ else None,
                 ctypes.c_void_p(j.data_ptr()) if np_ else None,
                 ctypes.c_void_p(S.data_ptr()) if np_ else None,
                 ctypes.c_void_p(pos.data_ptr()) if pos.numel() else None,
                 ctypes.c_void_p(self._cell.ctypes.data), ctypes.c_void_p(self._pbc.ctypes.data),
-                self.cutoff)
-        with torch.cuda.device(pos.device):
-            _ext.check(self._lib.nbl_verlet_refresh(*args, None, 0, ctypes.byref(n), sp))
-            m = int(n.value)
-            dev = pos.device
-            bufs = {"i": torch.empty(m, dtype=torch.int32, device=dev),
-                    "j": torch.empty(m, dtype=torch.int32, device=dev),
-                    "D": torch.empty((m, 3), dtype=torch.float64, device=dev),
-                    "d": torch.empty(m, dtype=torch.float64, device=dev),
-                    "S": torch.empty((m, 3), dtype=torch.int32, device=dev)}
-            want = set(self.quantities)
-            o = _ext.Outputs()
-            o.first = bufs["i"].data_ptr() if "i" in want and m else None
-            o.second = bufs["j"].data_ptr() if "j" in want and m else None
-            o.distvec = bufs["D"].data_ptr() if "D" in want and m else None
-            o.absdist = bufs["d"].data_ptr() if "d" in want and m else None
-            o.shift = bufs["S"].data_ptr() if "S" in want and m else None
-            if m:
-                _ext.check(self._lib.nbl_verlet_refresh(*args, ctypes.byref(o), m,
-                                                        ctypes.byref(n), sp))
+                self.cutoff, ctypes.byref(o), np_, ctypes.byref(n), sp))
+        m = int(n.value)
+        bufs = {k: v[:m] for k, v in bufs.items()}
         out = [bufs[c] for c in self.quantities]
         return out[0] if len(out) == 1 else tuple(out)

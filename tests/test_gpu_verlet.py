@@ -58,3 +58,66 @@ def test_verlet_single_quantity_and_errors():
     assert d.dim() == 1 and bool((d < 2.0).all())
     with pytest.raises(ValueError):
         VerletList(cutoff=2.0, skin=-1.0, cell=np.eye(3))
+
+
+def test_verlet_refresh_call_paths():
+    """nbl_verlet_refresh counts only (out NULL), refuses a capacity below the
+    kept count, and gives the same rows whether it writes before (capacity >=
+    stored pairs) or after (capacity = kept) reading the count."""
+    import ctypes
+    import torch
+    from matscipy_neighbours import _matscipy_neighbours as _ext
+    from matscipy_neighbours import _workloads as W
+    from matscipy_neighbours.neighbours import neighbour_list
+    from matscipy_neighbours.verlet import _lib
+    lib = _lib()
+    w = W.fcc_bulk(reps=5)
+    pos = torch.from_numpy(np.ascontiguousarray(w["positions"])).cuda()
+    i, j, S = neighbour_list("ijS", positions=pos, cell=w["cell"], pbc=w["pbc"], cutoff=4.5,
+                             array_namespace=torch)
+    pos2 = pos + torch.from_numpy(np.random.default_rng(2).normal(0, 0.05, pos.shape)).cuda()
+    cell = np.ascontiguousarray(w["cell"], dtype=np.float64)
+    pbc = np.ones(3, dtype=np.uint8)
+    npairs = int(i.shape[0])
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = ctypes.c_void_p
+
+    def call(o, cap):
+        n = ctypes.c_int64()
+        st = lib.nbl_verlet_refresh(npairs, P(i.data_ptr()), P(j.data_ptr()), P(S.data_ptr()),
+                                    P(pos2.data_ptr()), P(cell.ctypes.data), P(pbc.ctypes.data),
+                                    4.0, o, cap, ctypes.byref(n), sp)
+        return st, int(n.value)
+
+    st, kept = call(None, 0)
+    assert st == 0 and 0 < kept < npairs
+
+    def outputs(m):
+        t = {"i": torch.empty(m, dtype=torch.int32, device="cuda"),
+             "j": torch.empty(m, dtype=torch.int32, device="cuda"),
+             "D": torch.empty((m, 3), dtype=torch.float64, device="cuda"),
+             "d": torch.empty(m, dtype=torch.float64, device="cuda"),
+             "S": torch.empty((m, 3), dtype=torch.int32, device="cuda")}
+        o = _ext.Outputs()
+        o.first, o.second = t["i"].data_ptr(), t["j"].data_ptr()
+        o.distvec, o.absdist, o.shift = t["D"].data_ptr(), t["d"].data_ptr(), t["S"].data_ptr()
+        return t, o
+
+    t_small, o_small = outputs(kept - 1)
+    st, n = call(ctypes.byref(o_small), kept - 1)
+    assert st == _ext.NBL_ERROR_CAPACITY and n == kept
+    t_exact, o_exact = outputs(kept)
+    st, n = call(ctypes.byref(o_exact), kept)
+    assert st == 0 and n == kept
+    t_all, o_all = outputs(npairs)
+    st, n = call(ctypes.byref(o_all), npairs)
+    assert st == 0 and n == kept
+    torch.cuda.synchronize()
+    for k in "ijDdS":
+        assert torch.equal(t_exact[k], t_all[k][:kept])
+    # the kept rows are the stored rows with d < cutoff, in the stored order
+    D = pos2[j.long()] - pos2[i.long()] + S.double() @ torch.from_numpy(cell).cuda()
+    keep = (D * D).sum(1) < 16.0
+    assert torch.equal(t_all["i"][:kept], i[keep]) and torch.equal(t_all["j"][:kept], j[keep])
+    assert torch.equal(t_all["S"][:kept], S[keep])
