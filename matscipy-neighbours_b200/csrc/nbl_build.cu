@@ -344,7 +344,7 @@ constexpr int kPosTab = 640;     // pairs per window with a position table (fill
 static_assert(kRange <= 8192 && kITile <= 32,
               "position-table entries hold the candidate in 13 bits, the atom in 5");
 
-// Per-warp fill state, about 9.3 KB, so that six 4-warp CTAs fit an SM
+// Per-warp fill state, about 9.6 KB, so that five 4-warp CTAs fit an SM
 // (the force sink's sums live in a separate array of the force-sink kernel).
 template <bool FP32>
 struct __align__(16) FillSmem {
@@ -353,6 +353,7 @@ struct __align__(16) FillSmem {
     int4 iaux[kITile];
     int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     long long icur[kITile];
+    long long abase[kITile];   // output slot of window position 0 of each window atom
     uint32_t mw[kWinWords];
     int32_t mpre[kWinWords + 1];
     union {
@@ -361,14 +362,12 @@ struct __align__(16) FillSmem {
     };
     uint8_t cand_seg[kCandTab];     // segment of each of the batch's first candidates
 };
-static_assert(4 * sizeof(FillSmem<true>) <= 37888 && 4 * sizeof(FillSmem<false>) <= 37888,
-              "six fill CTAs per SM: at most 37 KB of shared memory per CTA");
+static_assert(5 * (4 * sizeof(FillSmem<true>) + 4 * 32 * 32 + 1024) <= 233472 &&
+                  5 * (4 * sizeof(FillSmem<false>) + 4 * 32 * 32 + 1024) <= 233472,
+              "five fill CTAs per SM (force-sink sums included) fit the SM's shared memory");
 
 // Resident CTAs per SM the fill is compiled for (registers and shared memory).
-template <bool LJ>
-struct FillOcc {
-    static constexpr int kBlocks = LJ ? 5 : 5;
-};
+constexpr int kFillBlocks = 5;
 
 // Per-home-cell constants kept in registers.
 struct Hot {
@@ -942,7 +941,7 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
             kk = kr + (lo - al * nch) * 32 + bit;
         }
         w.il = a0 + al;
-        w.slot = sm.icur[w.il] + (P - sm.mpre[al * nch]);
+        w.slot = sm.abase[al] + P;
         w.seg = seg_of_tab(sm, nseg, kk);
         const int32_t sj = sm.sg.b[w.seg] + (kk - sm.sg.pref[w.seg]);
         w.pj = a.pos64[sj];
@@ -1054,7 +1053,7 @@ __device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc
 }
 
 template <bool FP32, int KIND, bool LJ>
-__global__ void __launch_bounds__(kThreads, FillOcc<LJ>::kBlocks)
+__global__ void __launch_bounds__(kThreads, kFillBlocks)
 k_fill(TraverseArgs a) {
     constexpr int kCand = FillTile<FP32>::kCand;
     __shared__ FillSmem<FP32> smem[kWarps];
@@ -1119,9 +1118,9 @@ k_fill(TraverseArgs a) {
                     const int nch = (nrange + 31) >> 5;
                     const float inv_nch = 1.0f / (float)nch;
                     const int win = max(1, kWinWords / nch);
-                    for (int a0 = 0; a0 < ni; a0 += win) {
-                        const int na = min(win, ni - a0);
-                        const int nw = na * nch;
+                    for (int a0 = 0; a0 < ni;) {
+                        int na = min(win, ni - a0);
+                        int nw = na * nch;
                         // --- the window's hit words ---------------------------------
                         if (mbase >= 0) {
                             for (int w = lane; w < nw; w += 32) {
@@ -1165,6 +1164,19 @@ k_fill(TraverseArgs a) {
                         }
                         if (lane == 0) sm.mpre[nw] = carry;
                         __syncwarp();
+                        // --- a window over the position table keeps only the atoms
+                        //     whose pairs fit it (at least one); the next window
+                        //     starts at the first atom left out ---------------------
+                        if (carry > kPosTab && na > 1) {
+                            const bool fits = lane >= 1 && lane <= na &&
+                                              sm.mpre[lane * nch] <= kPosTab;
+                            na = max(1, __popc(__ballot_sync(full, fits)));
+                            nw = na * nch;
+                            carry = sm.mpre[nw];
+                        }
+                        // per-atom output base: slot = abase[atom] + window position
+                        if (lane < na) sm.abase[lane] = sm.icur[a0 + lane] - sm.mpre[lane * nch];
+                        __syncwarp();
                         // --- small windows: each word writes its bits' positions into
                         //     a table (lane = word, ffs over its set bits), so a lane
                         //     finds its pair with one shared-memory load --------------
@@ -1202,6 +1214,7 @@ k_fill(TraverseArgs a) {
                         if (lane < na)
                             sm.icur[a0 + lane] += sm.mpre[(lane + 1) * nch] - sm.mpre[lane * nch];
                         __syncwarp();
+                        a0 += na;
                     }
                 }
             }
