@@ -950,8 +950,9 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
     return w;
 }
 
-// Compute and store one pair (exact FP64 D and d, S, i, j).
-template <bool FP32>
+// Compute and store one pair (exact FP64 D and d, S, i, j).  ALL5: all five
+// outputs requested and no neighbour matrix (no per-pair output checks).
+template <bool FP32, bool ALL5>
 __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const TraverseArgs &a,
                                            const Hot &H, const PairWork &w) {
     if (!w.act) return;
@@ -962,7 +963,7 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
     const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
     const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
     const int32_t jl = (int32_t)(w.aj.x - H.atom_base);
-    if (a.mat_k > 0) {
+    if (!ALL5 && a.mat_k > 0) {
         const long long rank = w.slot - (long long)a.offsets[ai.x];
         if (rank < a.mat_k) {
             const long long m = (long long)ai.x * a.mat_k + rank;
@@ -978,19 +979,19 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
         atomicOr(a.err, kErrCapacity);
         return;
     }
-    if (a.first) __stcs(a.first + slot, (int32_t)(ai.x - H.atom_base));
-    if (a.second) __stcs(a.second + slot, jl);
-    if (a.absdist) {
+    if (ALL5 || a.first) __stcs(a.first + slot, (int32_t)(ai.x - H.atom_base));
+    if (ALL5 || a.second) __stcs(a.second + slot, jl);
+    if (ALL5 || a.absdist) {
         const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
         __stcs(a.absdist + slot, __dsqrt_rn(r2));
     }
-    if (a.distvec) {
+    if (ALL5 || a.distvec) {
         double *D = a.distvec + 3 * slot;
         __stcs(D, dx);
         __stcs(D + 1, dy);
         __stcs(D + 2, dz);
     }
-    if (a.shift) {
+    if (ALL5 || a.shift) {
         int32_t *Sv = a.shift + 3 * slot;
         __stcs(Sv, ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0]);
         __stcs(Sv + 1, ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1]);
@@ -1052,7 +1053,7 @@ __device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc
     __syncwarp();
 }
 
-template <bool FP32, int KIND, bool LJ>
+template <bool FP32, int KIND, bool LJ, bool ALL5>
 __global__ void __launch_bounds__(kThreads, kFillBlocks)
 k_fill(TraverseArgs a) {
     constexpr int kCand = FillTile<FP32>::kCand;
@@ -1207,7 +1208,7 @@ k_fill(TraverseArgs a) {
                             if (LJ)
                                 lj_round<FP32>(sm, facc, a, cur, lane);
                             else
-                                store_pair<FP32>(sm, a, H, cur);
+                                store_pair<FP32, ALL5>(sm, a, H, cur);
                             cur = nxt;
                         }
                         __syncwarp();
@@ -1243,8 +1244,8 @@ k_fill(TraverseArgs a) {
 #define NBL_INST(F, K)                                            \
     template __global__ void k_count<F, K, 2>(TraverseArgs);      \
     template __global__ void k_count<F, K, 4>(TraverseArgs);      \
-    template __global__ void k_fill<F, K, false>(TraverseArgs);   \
-    template __global__ void k_fill<F, K, true>(TraverseArgs);
+    template __global__ void k_fill<F, K, false, false>(TraverseArgs); \
+    template __global__ void k_fill<F, K, true, false>(TraverseArgs);
 NBL_INST(true, kCutScalar)
 NBL_INST(true, kCutPerAtom)
 NBL_INST(true, kCutPerType)
@@ -1252,6 +1253,9 @@ NBL_INST(false, kCutScalar)
 NBL_INST(false, kCutPerAtom)
 NBL_INST(false, kCutPerType)
 #undef NBL_INST
+template __global__ void k_fill<true, kCutScalar, false, true>(TraverseArgs);
+template __global__ void k_fill<true, kCutPerAtom, false, true>(TraverseArgs);
+template __global__ void k_fill<true, kCutPerType, false, true>(TraverseArgs);
 
 // One block per system with a visit table: its visited offsets in the
 // traversal's z/y/x order (neighbour_visit.hh:63-84).
@@ -1351,7 +1355,8 @@ template <bool F, int K>
 int occupancy_fk(int mode, int group, bool lj) {
     if (mode == kModeCount) return group == 2 ? occupancy_of(k_count<F, K, 2>)
                                               : occupancy_of(k_count<F, K, 4>);
-    return lj ? occupancy_of(k_fill<F, K, true>) : occupancy_of(k_fill<F, K, false>);
+    return lj ? occupancy_of(k_fill<F, K, true, false>)
+              : occupancy_of(k_fill<F, K, false, false>);
 }
 
 }  // namespace
@@ -1385,6 +1390,25 @@ int traverse_blocks_per_sm(int mode, bool fp32, int kind, int group, bool lj) {
     return n;
 }
 
+namespace {
+
+template <bool F, int K>
+void launch_fill(const TraverseArgs &a, int grid, cudaStream_t st) {
+    if (a.lj_force != nullptr) {
+        k_fill<F, K, true, false><<<grid, kThreads, 0, st>>>(a);
+        return;
+    }
+    if constexpr (F) {
+        if (a.first && a.second && a.distvec && a.absdist && a.shift && a.mat_k == 0) {
+            k_fill<F, K, false, true><<<grid, kThreads, 0, st>>>(a);
+            return;
+        }
+    }
+    k_fill<F, K, false, false><<<grid, kThreads, 0, st>>>(a);
+}
+
+}  // namespace
+
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, int group) {
     if (grid <= 0) return cudaSuccess;
@@ -1395,13 +1419,7 @@ cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a
         else                                                               \
             k_count<F, K, 4><<<grid, kThreads, 0, st>>>(a);                \
     } while (0)
-#define NBL_GO_F(F, K)                                                     \
-    do {                                                                   \
-        if (a.lj_force != nullptr)                                         \
-            k_fill<F, K, true><<<grid, kThreads, 0, st>>>(a);              \
-        else                                                               \
-            k_fill<F, K, false><<<grid, kThreads, 0, st>>>(a);             \
-    } while (0)
+#define NBL_GO_F(F, K) launch_fill<F, K>(a, grid, st)
 #define NBL_BY_KIND(GO, F)                            \
     do {                                              \
         if (kind == kCutPerAtom)                      \
