@@ -277,8 +277,15 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.i_hi = INT64_MAX;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = (int)std::min<int64_t>((int64_t)nsm * 6, std::max<int64_t>(N, 1));
-    NA_CUDA(launch_traverse(kModeCount, b.fp32, b.sys[0].cutoff_kind, ta, grid, s), "count pass");
+    // two whole waves of each pass's resident CTAs
+    const int kind = b.sys[0].cutoff_kind;
+    const int count_grid = (int)std::min<int64_t>(
+        (int64_t)nsm * 2 * std::max(1, traverse_blocks_per_sm(kModeCount, b.fp32, kind)),
+        std::max<int64_t>(N, 1));
+    const int fill_grid = (int)std::min<int64_t>(
+        (int64_t)nsm * 2 * std::max(1, traverse_blocks_per_sm(kModeFill, b.fp32, kind)),
+        std::max<int64_t>(N, 1));
+    NA_CUDA(launch_traverse(kModeCount, b.fp32, kind, ta, count_grid, s), "count pass");
     NA_CUDA(exclusive_scan_i32_i64(counts, N, offsets, scan64, s), "scan");
 
     // Pair count and error bits back through pageable host memory.
@@ -309,7 +316,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.absdist = out->absdist;
     ta.shift = out->shift;
     ta.capacity = capacity;
-    NA_CUDA(launch_traverse(kModeFill, b.fp32, b.sys[0].cutoff_kind, ta, grid, s), "fill pass");
+    NA_CUDA(launch_traverse(kModeFill, b.fp32, kind, ta, fill_grid, s), "fill pass");
 #undef NA_CUDA
     return NBL_SUCCESS;
 }
