@@ -250,7 +250,8 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_home = L.add(sizeof(HomeCell) * N);
     size_t o_cnt = L.add(sizeof(int32_t) * (N + 1));
     size_t o_off = L.add(sizeof(int64_t) * (N + 1));
-    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err, overflow, mask cursor
+    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err, overflow, items, mask cursor,
+                                              // item ticket
     const int64_t mask_cap = mask_words(p, b);
     size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
     size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1) * kMaskBatches);
@@ -527,6 +528,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.offsets = B.offsets;
     ta.mask_pool = B.mask_pool;
     ta.mask_cursor = reinterpret_cast<unsigned long long *>(B.small + 4);
+    ta.item_next = B.small + 6;
     ta.mask_cap = B.mask_cap;
     ta.home_mask = B.home_mask;
     ta.err = err;

@@ -675,6 +675,21 @@ __device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const Se
     }
 }
 
+// The warp's first work item: a ticket from a.item_next, else the warp index.
+__device__ __forceinline__ int first_item(const TraverseArgs &a, int gwarp, int lane) {
+    if (a.item_next == nullptr) return gwarp;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(a.item_next, 1);
+    return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// The warp's next work item: lane 0's ticket `pend` (claimed at the start of
+// the current item), else a fixed stride.
+__device__ __forceinline__ int next_item(const TraverseArgs &a, int it, int nwarps, int pend) {
+    if (a.item_next == nullptr) return it + nwarps;
+    return __shfl_sync(0xffffffffu, pend, 0);
+}
+
 // Position of the (r+1)-th set bit of w (r < popc(w)).
 __device__ __forceinline__ int nth_set_bit(unsigned w, int r) {
     int pos = 0;
@@ -714,7 +729,10 @@ k_count(TraverseArgs a) {
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    for (int it = gwarp; it < nitems; it += nwarps) {
+    int pend = 0;  // lane 0: the ticket claimed while the current item runs
+    for (int it = first_item(a, gwarp, lane); it < nitems;
+         it = next_item(a, it, nwarps, pend)) {
+        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
         const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
         const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
@@ -1067,7 +1085,10 @@ k_fill(TraverseArgs a) {
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    for (int it = gwarp; it < nitems; it += nwarps) {
+    int pend = 0;  // lane 0: the ticket claimed while the current item runs
+    for (int it = first_item(a, gwarp, lane); it < nitems;
+         it = next_item(a, it, nwarps, pend)) {
+        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
         const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
         const Home c = load_home<FP32>(a, item.x);
         const Hot &H = c.H;
@@ -1412,6 +1433,10 @@ void launch_fill(const TraverseArgs &a, int grid, cudaStream_t st) {
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, int group) {
     if (grid <= 0) return cudaSuccess;
+    if (a.item_next != nullptr) {
+        const cudaError_t e = cudaMemsetAsync(a.item_next, 0, sizeof(int), st);
+        if (e != cudaSuccess) return e;
+    }
 #define NBL_GO_C(F, K)                                                     \
     do {                                                                   \
         if (group == 2)                                                    \

@@ -100,6 +100,10 @@ struct TraverseArgs {
     // as i; every atom stays a candidate j.  Rows outside keep count 0.
     long long i_lo;
     long long i_hi;
+    // Work-item ticket (one int, zeroed by launch_traverse before each pass):
+    // each warp claims its next item with one atomic, so warps that drew
+    // cheap items take more.  NULL: a fixed warp stride over the items.
+    int *item_next;
 };
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);

@@ -273,6 +273,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.counts = counts;
     ta.offsets = offsets;
     ta.err = small + 1;
+    ta.item_next = small + 6;
     ta.i_lo = 0;
     ta.i_hi = INT64_MAX;
     int nsm = 148;

@@ -55,7 +55,7 @@ struct Bufs {
     int64_t *offsets = nullptr;
     int *small = nullptr;  // [0] occupied cells, [1] error bits, [2] matrix
                            // overflow, [3] work items, [4..5] mask-pool cursor
-                           // (u64)
+                           // (u64), [6] work-item ticket of the pair passes
     uint32_t *mask_pool = nullptr;
     long long mask_cap = 0;
     long long *home_mask = nullptr;
