@@ -274,8 +274,9 @@ cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *ta
 // ---------------------------------------------------------------------------
 //
 // Both take one work item (home cell x i-tile of up to 32 atoms) per WARP
-// (warp-strided over the work list; a CTA is four independent warps, so there
-// is no block-wide barrier).  Per item, one lane per visited neighbour offset
+// (each warp claims its next item with an atomic ticket, issued while the
+// current item runs; a CTA is four independent warps, so there is no
+// block-wide barrier).  Per item, one lane per visited neighbour offset
 // reads the offset vector (FP64, reference order, from the per-system visit
 // table), the wrap counts and the cell slice, and a warp scan turns slice
 // lengths into candidate positions (the "segment batch").
