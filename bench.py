@@ -165,6 +165,7 @@ def batched_bench(steps, warmup, dev, rank=0):
         ms.append(e0.elapsed_time(e1))
     b.finish()
     cfg = b.config()
+    tickets = b.tickets()
     positions = b.positions
     offs = b.atom_offsets
     b.close()
@@ -223,7 +224,9 @@ def batched_bench(steps, warmup, dev, rank=0):
                                    "ms_per_step": batched_s * 1e3,
                                    "launch_config": {"count_ctas_per_sm": cfg[0],
                                                      "count_atoms_per_pass": cfg[1],
-                                                     "fill_ctas_per_sm": cfg[2]}},
+                                                     "fill_ctas_per_sm": cfg[2],
+                                                     "count_item_tickets": tickets[0],
+                                                     "fill_item_tickets": tickets[1]}},
             "plain_fp64_per_system": {"value": npairs / plain_s, "unit": UNIT,
                                       "ms_per_step": plain_s * 1e3},
             "speedup": plain_s / batched_s}

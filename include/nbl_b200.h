@@ -273,6 +273,10 @@ NBL_API nbl_status nbl_batch_get_outputs(nbl_batch *batch, nbl_batch_outputs *ou
 /* The launch configuration in use (chosen by the autotuner when enabled). */
 NBL_API nbl_status nbl_batch_get_config(nbl_batch *batch, int *count_mult,
                                         int *count_group, int *fill_mult);
+/* Whether the count and fill passes hand work items out by atomic ticket (1)
+   or by a fixed warp stride (0), as the autotuner chose. */
+NBL_API nbl_status nbl_batch_get_tickets(nbl_batch *batch, int *count_tickets,
+                                         int *fill_tickets);
 
 /* ---- backward: gradients through the pair list -------------------------
    (Build-only form with no reference counterpart.)  For a fixed pair list of

@@ -528,7 +528,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.offsets = B.offsets;
     ta.mask_pool = B.mask_pool;
     ta.mask_cursor = reinterpret_cast<unsigned long long *>(B.small + 4);
-    ta.item_next = B.small + 6;
+    ta.item_next = p.count_tickets ? B.small + 6 : nullptr;
     ta.mask_cap = B.mask_cap;
     ta.home_mask = B.home_mask;
     ta.err = err;
@@ -581,6 +581,7 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     if (!p.have_count)
         return set_error(NBL_ERROR_INVALID_ARGUMENT, "nbl_fill without a preceding nbl_count");
     TraverseArgs ta = p.targs;
+    ta.item_next = p.fill_tickets ? p.bufs.small + 6 : nullptr;
     ta.first = o.first;
     ta.second = o.second;
     ta.distvec = o.distvec;
@@ -870,6 +871,7 @@ nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
     NBL_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t) * n, st), "memset matrix");
     NBL_CUDA(cudaMemsetAsync(p.bufs.small + 2, 0, sizeof(int), st), "memset flag");
     TraverseArgs ta = p.targs;
+    ta.item_next = p.fill_tickets ? p.bufs.small + 6 : nullptr;
     ta.mat_k = max_neighbours;
     ta.mat_idx = idx;
     ta.mat_dist = dist;
@@ -912,6 +914,7 @@ nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
         return NBL_SUCCESS;
     }
     TraverseArgs ta = p.targs;
+    ta.item_next = p.fill_tickets ? p.bufs.small + 6 : nullptr;
     ta.first = ta.second = nullptr;
     ta.distvec = ta.absdist = nullptr;
     ta.shift = nullptr;

@@ -47,7 +47,7 @@ __global__ void k_sys_offsets(const int64_t *__restrict__ offsets,
 }
 
 struct TuneChoice {
-    int count_mult, count_group, fill_mult;
+    int count_mult, count_group, fill_mult, count_tickets, fill_tickets;
 };
 
 std::mutex g_tune_mutex;
@@ -63,8 +63,8 @@ void tune_load_locked() {
     if (!f) return;
     char key[256];
     TuneChoice c;
-    while (std::fscanf(f, "%255s %d %d %d", key, &c.count_mult, &c.count_group,
-                       &c.fill_mult) == 4)
+    while (std::fscanf(f, "%255s %d %d %d %d %d", key, &c.count_mult, &c.count_group,
+                       &c.fill_mult, &c.count_tickets, &c.fill_tickets) == 6)
         g_tune_cache[key] = c;
     std::fclose(f);
 }
@@ -75,7 +75,8 @@ void tune_store_locked(const std::string &key, const TuneChoice &c) {
     if (!path) return;
     FILE *f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d\n", key.c_str(), c.count_mult, c.count_group, c.fill_mult);
+    std::fprintf(f, "%s %d %d %d %d %d\n", key.c_str(), c.count_mult, c.count_group,
+                 c.fill_mult, c.count_tickets, c.fill_tickets);
     std::fclose(f);
 }
 
@@ -235,7 +236,7 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         max_visit = std::max(max_visit, b.sys[s].nvisit);
     }
     char key[160];
-    std::snprintf(key, sizeof(key), "w2_sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
+    std::snprintf(key, sizeof(key), "w3_sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
                   b.sys.empty() ? 0 : b.sys[0].cutoff_kind, b.fp32 ? 1 : 0,
                   bucket_log2(b.natoms / std::max(cells, 1.0)), bucket_log2(max_visit));
     bt->tune_key = key;
@@ -247,13 +248,16 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
             bt->p.count_mult = it->second.count_mult;
             bt->p.count_group = it->second.count_group;
             bt->p.fill_mult = it->second.fill_mult;
+            bt->p.count_tickets = it->second.count_tickets != 0;
+            bt->p.fill_tickets = it->second.fill_tickets != 0;
             return NBL_SUCCESS;
         }
     }
     cudaEvent_t e0, e1;
     NBL_CUDA(cudaEventCreate(&e0), "event");
     NBL_CUDA(cudaEventCreate(&e1), "event");
-    TuneChoice best{bt->p.count_mult, bt->p.count_group, bt->p.fill_mult};
+    TuneChoice best{bt->p.count_mult, bt->p.count_group, bt->p.fill_mult,
+                    bt->p.count_tickets ? 1 : 0, bt->p.fill_tickets ? 1 : 0};
     float best_ms = 1e30f;
     // grids of 1, 2 and 4 full waves of each kernel's resident CTAs
     const int waves[] = {1, 2, 4};
@@ -263,19 +267,24 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         if (!b.fp32 && g != 4) continue;  // the group only shapes the FP32 sweep
         const int occ = std::max(1, traverse_blocks_per_sm(kModeCount, b.fp32, kind, g));
         for (int wv : waves) {
-            const int m = wv * occ;
-            bt->p.count_mult = m;
-            bt->p.count_group = g;
-            const float ms = time_count(bt, st, e0, e1);
-            if (ms < best_ms) {
-                best_ms = ms;
-                best.count_mult = m;
-                best.count_group = g;
+            for (int tk = 1; tk >= 0; tk--) {
+                const int m = wv * occ;
+                bt->p.count_mult = m;
+                bt->p.count_group = g;
+                bt->p.count_tickets = tk != 0;
+                const float ms = time_count(bt, st, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.count_mult = m;
+                    best.count_group = g;
+                    best.count_tickets = tk;
+                }
             }
         }
     }
     bt->p.count_mult = best.count_mult;
     bt->p.count_group = best.count_group;
+    bt->p.count_tickets = best.count_tickets != 0;
     if (enqueue_count(bt->p, bt->b, st) != NBL_SUCCESS) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -285,22 +294,27 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
     best_ms = 1e30f;
     const int focc = std::max(1, traverse_blocks_per_sm(kModeFill, b.fp32, kind));
     for (int wv : waves) {
-        const int m = wv * focc;
-        bt->p.fill_mult = m;
-        bt->p.fill_grid = std::max(1, std::min(bt->p.num_sms * m, (int)std::max<int64_t>(
-                                                                    (b.natoms + 3) / 4, 1)));
-        const float ms = time_fill(bt, st, e0, e1);
-        if (ms >= 1e30f) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return NBL_ERROR_INTERNAL;
-        }
-        if (ms < best_ms) {
-            best_ms = ms;
-            best.fill_mult = m;
+        for (int tk = 1; tk >= 0; tk--) {
+            const int m = wv * focc;
+            bt->p.fill_mult = m;
+            bt->p.fill_tickets = tk != 0;
+            bt->p.fill_grid = std::max(1, std::min(bt->p.num_sms * m, (int)std::max<int64_t>(
+                                                                        (b.natoms + 3) / 4, 1)));
+            const float ms = time_fill(bt, st, e0, e1);
+            if (ms >= 1e30f) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return NBL_ERROR_INTERNAL;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.fill_mult = m;
+                best.fill_tickets = tk;
+            }
         }
     }
     bt->p.fill_mult = best.fill_mult;
+    bt->p.fill_tickets = best.fill_tickets != 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -537,6 +551,13 @@ NBL_API nbl_status nbl_batch_get_config(nbl_batch *bt, int *count_mult, int *cou
     if (count_mult) *count_mult = bt->p.count_mult;
     if (count_group) *count_group = bt->p.count_group;
     if (fill_mult) *fill_mult = bt->p.fill_mult;
+    return NBL_SUCCESS;
+}
+
+NBL_API nbl_status nbl_batch_get_tickets(nbl_batch *bt, int *count_tickets, int *fill_tickets) {
+    if (!bt) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null batch");
+    if (count_tickets) *count_tickets = bt->p.count_tickets ? 1 : 0;
+    if (fill_tickets) *fill_tickets = bt->p.fill_tickets ? 1 : 0;
     return NBL_SUCCESS;
 }
 

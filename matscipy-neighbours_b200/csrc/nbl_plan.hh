@@ -88,6 +88,9 @@ struct Plan {
     int count_mult = 0;
     int fill_mult = 0;
     int count_group = 4;
+    // Work items by atomic ticket (else a fixed warp stride) in each pass.
+    bool count_tickets = true;
+    bool fill_tickets = true;
     int64_t mask_hint = 0;    // mask-pool words the last count asked for
     // Row range of nbl_set_atom_range (global atom indices, [lo, hi)).
     int64_t i_lo = 0;

@@ -56,6 +56,8 @@ def _sigs():
         "nbl_batch_get_config": ([P, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "nbl_batch_get_tickets": ([P, ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     }
     for name, (args, res) in table.items():
         fn = getattr(lib, name)
@@ -242,6 +244,12 @@ class NeighbourListBatch:
         _ext.check(self._lib.nbl_batch_get_config(self._h, ctypes.byref(a), ctypes.byref(b),
                                                   ctypes.byref(c)))
         return a.value, b.value, c.value
+
+    def tickets(self):
+        """(count pass, fill pass) hand out work items by atomic ticket."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _ext.check(self._lib.nbl_batch_get_tickets(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return bool(a.value), bool(b.value)
 
     # -- results -----------------------------------------------------------
     def _tensor(self, ch):

@@ -101,6 +101,7 @@ def test_batch_autotune_picks_a_config(oracle):
     cm, grp, fm = b.config()
     # CTAs per SM: 1, 2 or 4 waves of each kernel's resident CTAs
     assert 1 <= cm <= 64 and grp in (2, 4) and 1 <= fm <= 64
+    assert all(isinstance(t, bool) for t in b.tickets())
     b.run()
     _check(oracle, b, systems)
     b.close()
