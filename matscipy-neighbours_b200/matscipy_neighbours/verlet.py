@@ -89,7 +89,9 @@ class VerletList:
 
     def update(self, positions):
         """The pairs within `cutoff` at `positions`, as a tuple in the order of
-        `quantities` (a bare tensor for one character)."""
+        `quantities` (a bare tensor for one character).  The tensors are views
+        of the first rows of buffers sized for the stored (cutoff + skin)
+        pairs, so that one device call writes them and reads the count."""
         torch = _ext._torch()
         pos = _ext.import_device_positions(positions)
         if self._stored is None or pos.shape[0] != self._ref.shape[0]:
