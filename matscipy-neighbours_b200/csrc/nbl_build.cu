@@ -7,9 +7,11 @@
 //   k_gather    per sorted atom: bin-relative position (FP64, reference
 //               arithmetic), its FP32 copy, image indices, cell slices,
 //               occupied-cell work list
-//   k_traverse<COUNT>  per occupied home cell: neighbour counts per atom
+//   k_tiles     occupied cells -> work items (home cell x i-tile of <= 32 atoms)
+//   k_visit     per system: the visited cell offsets' vectors (reference order)
+//   k_count     per work item: neighbour counts per atom, hit words
 //   scan        (nbl_sort.cu) counts -> row offsets, total pair count
-//   k_traverse<FILL>   per occupied home cell: writes i, j, D, d, S
+//   k_fill      per work item: writes i, j, D, d, S (or feeds a force sink)
 //
 // The traversal reproduces neighbour_visit.hh:51-120 exactly: the same
 // visited offsets in the same z/y/x order, the same cell slices in ascending
@@ -18,13 +20,12 @@
 // including the order of pairs within a row.
 //
 // Work decomposition (instead of the reference's thread-per-atom loop): one
-// CTA per occupied home cell.  The CTA enumerates the visited neighbour cells
-// ("segments"), stages their atoms ("candidates") in shared memory, and each
-// warp takes one atom i of the home cell and sweeps the candidates 32 at a
-// time: FP32 distance filter (or plain FP64), __ballot_sync + __popc for the
-// count, and in the fill pass the hits go into a per-warp queue that is
-// drained 32 pairs at a time so that the FP64 epilogue and the stores run
-// with full warps and near-contiguous addresses.
+// warp per work item, the item's visited neighbour cells ("segments") one per
+// lane, their atoms ("candidates") staged in shared memory; the count sweeps
+// them 32 at a time against the tile's atoms (FP32 filter with an FP64 guard
+// band, or plain FP64; __ballot_sync + __popc), and the fill turns the hit
+// words into 32 pairs per round so that the FP64 epilogue and the stores run
+// with full warps and near-contiguous addresses (details below).
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -289,11 +290,11 @@ cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *ta
 // pool, stored as one 32-bit word per (atom, chunk).
 //
 // k_fill turns hit words back into pairs lane-parallel: for a window of atoms
-// it builds the prefix of the words' popcounts; for windows of up to kPosTab
-// pairs each word then writes its set bits' (candidate, atom) codes at their
-// output positions (lane = word, ffs), so lane L of each round finds pair
-// P = P0 + L with one shared-memory load (larger windows search: binary
-// search over the prefix, then an n-th-set-bit search).  The pair (exact FP64
+// it builds the prefix of the words' popcounts and keeps the atoms whose pairs
+// fit kPosTab; each word then writes its set bits' (candidate, atom) codes at
+// their output positions (lane = word, ffs), so lane L of each round finds
+// pair P = P0 + L with one shared-memory load (a single atom with more pairs
+// searches: binary search over the prefix, then an n-th-set-bit search).  The pair (exact FP64
 // D, d and S) goes to row_start + rank, so consecutive lanes write
 // consecutive slots; the next round's j-side loads are issued before this
 // round's stores.  Items without pool words (pool full, more than one segment
