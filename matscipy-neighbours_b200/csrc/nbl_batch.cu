@@ -11,11 +11,12 @@
 // reports (with the true count, so the caller can set up a larger batch).
 //
 // Autotuner: the pair passes' launch configuration -- CTAs per SM of the count
-// and fill kernels, and how many atoms the FP32 count sweeps per pass over a
-// candidate tile -- is timed on the batch itself at set-up and the fastest
-// choice is cached per (SM count, cutoff kind, precision, atoms-per-cell
-// bucket, visited-cells bucket), in memory and, when NBL_TUNE_CACHE names a
-// file, on disk.
+// and fill kernels (1, 2 or 4 waves of their resident CTAs), work items by
+// atomic ticket or by fixed stride in each, and how many atoms the FP32 count
+// sweeps per pass over a candidate tile -- is timed on the batch itself at
+// set-up and the fastest choice is cached per (SM count, cutoff kind,
+// precision, atoms-per-cell bucket, visited-cells bucket), in memory and, when
+// NBL_TUNE_CACHE names a file, on disk.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
