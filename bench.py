@@ -52,6 +52,54 @@ def _env_int(name, default):
         return default
 
 
+def _workloads():
+    """The seeded workload generators, loaded from their own file: importing
+    them through the package would run its __init__, which loads the engine's
+    CUDA library, and the reference arm must run without any engine code in
+    the process."""
+    import importlib.util
+    name = "nbl_bench_workloads"
+    if name not in sys.modules:
+        path = ROOT / "matscipy-neighbours_b200" / "matscipy_neighbours" / "_workloads.py"
+        spec = importlib.util.spec_from_file_location(name, path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def _oracle():
+    """The CPU checker (oracle/): the reference's own core when it was built
+    (oracle/_ref), else the C restatement."""
+    if str(ROOT / "oracle") not in sys.path:
+        sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    return O
+
+
+def _same(got, want):
+    """Bit-identical arrays (floats compared by their bit patterns)."""
+    import numpy as np
+    got = np.asarray(got)
+    want = np.asarray(want)
+    if got.shape != want.shape or got.dtype != want.dtype:
+        return False
+    if got.dtype.kind == "f":
+        return bool(np.array_equal(got.view(np.int64), want.view(np.int64)))
+    return bool(np.array_equal(got, want))
+
+
+def _same_device(quantities, dev_arrays, want):
+    """Engine outputs (torch device tensors, one per quantity) against the
+    checker's host arrays, one quantity at a time (bounded host memory)."""
+    if len(quantities) == 1:
+        want = (want,)
+    for q, t, w in zip(quantities, dev_arrays, want):
+        if not _same(t.cpu().numpy(), w):
+            return False
+    return True
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -132,27 +180,13 @@ class ClockSampler:
                 "samples": len(self.samples), "source": "nvml, 20 ms"}
 
 
-def batched_bench(steps, warmup, dev, rank=0):
-    """C4: 4,096 small systems (sizes log-uniform 8-512, random triclinic cells
-    scaled towards 0.08 A^-3, random pbc, per-atom radii 3-6 A, ijdDS).
-    Batched: the FP32-filter build of all systems replayed from one captured
-    CUDA graph.  Plain: one FP64 nbl_count + nbl_fill per system."""
-    import ctypes
-
-    import numpy as np
+def _time_batch(b, steps, warmup):
+    """Median device time (ms) of `steps` replays of a batch's graph, each
+    bracketed by CUDA events on the batch's stream."""
     import torch
-
-    from matscipy_neighbours import _matscipy_neighbours as ext
-    from matscipy_neighbours import _workloads as W
-    from matscipy_neighbours.batch import NeighbourListBatch
-
-    systems = W.batched_systems(seed=1 + rank)
-    b = NeighbourListBatch(systems, precision="fp32", graph=True, autotune=True,
-                           device=dev.index)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.current_stream(b.device)
     for _ in range(warmup):
         b.run()
-    npairs = b.npairs
     ms = []
     for _ in range(steps):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -164,6 +198,50 @@ def batched_bench(steps, warmup, dev, rank=0):
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     b.finish()
+    return statistics.median(ms)
+
+
+def batched_bench(steps, warmup, dev, rank=0, check=False):
+    """C4: 4,096 small systems (sizes log-uniform 8-512, random triclinic cells
+    scaled towards 0.08 A^-3, random pbc, per-atom radii 3-6 A, ijdDS).
+    Batched: the FP32-filter build of all systems replayed from one captured
+    CUDA graph, and the same graph with the plain FP64 test (the precision
+    gain alone).  Plain: one FP64 nbl_count + nbl_fill per system (the
+    batching gain on top).  With `check`, every system's output is compared
+    bit for bit with the CPU checker run on that system alone."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    from matscipy_neighbours.batch import NeighbourListBatch
+    W = _workloads()
+
+    systems = W.batched_systems(seed=1 + rank)
+    b64 = NeighbourListBatch(systems, precision="fp64", graph=True, autotune=True,
+                             device=dev.index)
+    fp64_ms = _time_batch(b64, steps, warmup)
+    cfg64 = b64.config()
+    b64.close()
+    b = NeighbourListBatch(systems, precision="fp32", graph=True, autotune=True,
+                           device=dev.index)
+    stream = torch.cuda.current_stream(dev)
+    batched_ms = _time_batch(b, steps, warmup)
+    npairs = b.npairs
+    parity = None
+    if check:
+        O = _oracle()
+        _, _, fn = _cpu_fn(O, len(os.sched_getaffinity(0)))
+        off = b.sys_offsets()
+        res = [t.cpu().numpy() for t in b.results()]
+        parity = True
+        for s, sd in enumerate(systems):
+            want = fn("ijdDS", sd["cell"], sd["positions"], sd["cutoff"], sd["pbc"])
+            if not all(_same(r[off[s]:off[s + 1]], w) for r, w in zip(res, want)):
+                parity = False
+                break
+        del res
     cfg = b.config()
     tickets = b.tickets()
     positions = b.positions
@@ -217,22 +295,33 @@ def batched_bench(steps, warmup, dev, rank=0):
     torch.cuda.synchronize(dev)
     plain_s = time.perf_counter() - t0
     assert tot == npairs, (tot, npairs)
-    batched_s = statistics.median(ms) * 1e-3
-    return {"workload": "batched_4096_systems", "systems": len(systems),
-            "atoms": int(offs[-1]), "npairs": int(npairs),
-            "batched_fp32_graph": {"value": npairs / batched_s, "unit": UNIT,
-                                   "ms_per_step": batched_s * 1e3,
-                                   "launch_config": {"count_ctas_per_sm": cfg[0],
-                                                     "count_atoms_per_pass": cfg[1],
-                                                     "fill_ctas_per_sm": cfg[2],
-                                                     "count_item_tickets": tickets[0],
-                                                     "fill_item_tickets": tickets[1]}},
-            "plain_fp64_per_system": {"value": npairs / plain_s, "unit": UNIT,
-                                      "ms_per_step": plain_s * 1e3},
-            "speedup": plain_s / batched_s}
+    batched_s = batched_ms * 1e-3
+    out = {"workload": "batched_4096_systems", "systems": len(systems),
+           "atoms": int(offs[-1]), "npairs": int(npairs),
+           "batched_fp32_graph": {"value": npairs / batched_s, "unit": UNIT,
+                                  "ms_per_step": batched_ms,
+                                  "launch_config": {"count_ctas_per_sm": cfg[0],
+                                                    "count_atoms_per_pass": cfg[1],
+                                                    "fill_ctas_per_sm": cfg[2],
+                                                    "count_item_tickets": tickets[0],
+                                                    "fill_item_tickets": tickets[1]}},
+           "batched_fp64_graph": {"value": npairs / (fp64_ms * 1e-3), "unit": UNIT,
+                                  "ms_per_step": fp64_ms,
+                                  "launch_config": {"count_ctas_per_sm": cfg64[0],
+                                                    "fill_ctas_per_sm": cfg64[2]}},
+           "plain_fp64_per_system": {"value": npairs / plain_s, "unit": UNIT,
+                                     "ms_per_step": plain_s * 1e3,
+                                     "note": "one nbl_count + nbl_fill per system, host "
+                                             "wall clock (4,096 synchronising calls)"},
+           "speedup": plain_s / batched_s,
+           "speedup_precision_only": fp64_ms / batched_ms,
+           "speedup_batching_only": plain_s / (fp64_ms * 1e-3)}
+    if parity is not None:
+        out["parity"] = parity
+    return out
 
 
-def configs_bench(dev, flush, reps=10, only=None):
+def configs_bench(dev, flush, reps=10, only=None, check=False):
     """The other configurations beside the headline (rank 0, N = 1): C1 plain
     small, C3 sparse slab (per-type cutoffs, ijdD), C5 differentiation lattice.
     Each: positions resident on the device, median of `reps` full builds
@@ -245,10 +334,9 @@ def configs_bench(dev, flush, reps=10, only=None):
     import numpy as np
     import torch
 
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
+    O = _oracle()
+    W = _workloads()
     from matscipy_neighbours import _matscipy_neighbours as ext
-    from matscipy_neighbours import _workloads as W
     from matscipy_neighbours.autograd import BackwardArgs, _lib
 
     peak, peak_kind, _ = _peaks()
@@ -281,47 +369,76 @@ def configs_bench(dev, flush, reps=10, only=None):
         types = w.get("numbers")
         types = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
         pos = torch.from_numpy(np.ascontiguousarray(w["positions"])).to(dev)
-        req = ext.make_request(flags, origin, cell, inv, pbc8, nat,
-                               ctypes.c_void_p(pos.data_ptr()), True, rc, pa, pt, nc,
-                               types, dev.index)
+        grids = ["auto"] + (["dense", "morton", "hashed"] if name.startswith("C3") else [])
         n = ctypes.c_int64()
-        ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
-        npairs = int(n.value)
-        bufs = {"i": torch.empty(npairs, dtype=torch.int32, device=dev),
-                "j": torch.empty(npairs, dtype=torch.int32, device=dev),
-                "D": torch.empty((npairs, 3), dtype=torch.float64, device=dev),
-                "d": torch.empty(npairs, dtype=torch.float64, device=dev),
-                "S": torch.empty((npairs, 3), dtype=torch.int32, device=dev)}
-        o = ext._outputs_struct({c: bufs[c] for c in q}, lambda t: t.data_ptr())
-        ms = []
-        for k in range(reps + 3):
-            flush.zero_()
-            torch.cuda.synchronize(dev)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+        bufs = None
+        grid_rows = {}
+        for grid in grids:
+            prev = ext.set_options(grid=grid)
+            req = ext.make_request(flags, origin, cell, inv, pbc8, nat,
+                                   ctypes.c_void_p(pos.data_ptr()), True, rc, pa, pt, nc,
+                                   types, dev.index)
+            ext.set_options(grid=prev["grid"])
             ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
-            ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sptr))
-            e1.record(stream)
-            e1.synchronize()
-            if k >= 3:
-                ms.append(e0.elapsed_time(e1))
-        ext.check(ext.lib.nbl_check(plan, sptr))
-        gpu_s = statistics.median(ms) * 1e-3
+            npairs = int(n.value)
+            if bufs is None:
+                bufs = {"i": torch.empty(npairs, dtype=torch.int32, device=dev),
+                        "j": torch.empty(npairs, dtype=torch.int32, device=dev),
+                        "D": torch.empty((npairs, 3), dtype=torch.float64, device=dev),
+                        "d": torch.empty(npairs, dtype=torch.float64, device=dev),
+                        "S": torch.empty((npairs, 3), dtype=torch.int32, device=dev)}
+                o = ext._outputs_struct({c: bufs[c] for c in q}, lambda t: t.data_ptr())
+            ms, cms, fms = [], [], []
+            for k in range(reps + 3):
+                flush.zero_()
+                torch.cuda.synchronize(dev)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e2 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr, ctypes.byref(n)))
+                e1.record(stream)
+                ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sptr))
+                e2.record(stream)
+                e2.synchronize()
+                if k >= 3:
+                    ms.append(e0.elapsed_time(e2))
+                    cms.append(e0.elapsed_time(e1))
+                    fms.append(e1.elapsed_time(e2))
+            ext.check(ext.lib.nbl_check(plan, sptr))
+            grid_rows[grid] = (statistics.median(ms), statistics.median(cms),
+                               statistics.median(fms))
+        gpu_ms, count_ms, fill_ms = grid_rows["auto"]
+        gpu_s = gpu_ms * 1e-3
         cpu_args = (q, w["cell"], w["positions"], w["cutoff"], w["pbc"])
         cpu_fn(*cpu_args, types=types)
         ct = []
         for _ in range(3):
             t0 = time.perf_counter()
-            cpu_fn(*cpu_args, types=types)
+            res = cpu_fn(*cpu_args, types=types)
             ct.append(time.perf_counter() - t0)
         cpu_s = statistics.median(ct)
+        # algorithmic bytes of the whole build: the outputs plus the inputs
+        bq = sum({"i": 4, "j": 4, "D": 24, "d": 8, "S": 12}[c] for c in set(q))
+        bin_ = 24 + (8 if pa is not None else 0) + (4 if types is not None else 0)
+        alg = npairs * bq + nat * bin_
         row = {"natoms": nat, "npairs": npairs, "quantities": q,
-               "gpu_ms": gpu_s * 1e3, "gpu_pairs_per_s": npairs / gpu_s,
+               "gpu_ms": gpu_ms, "gpu_pairs_per_s": npairs / gpu_s,
+               "stage_ms": {"count_phase": count_ms, "fill": fill_ms},
+               "algorithmic_bytes": alg,
+               "hbm_frac_whole_build": alg / gpu_s / 1e9 / peak,
+               "hbm_frac_fill": alg / (fill_ms * 1e-3) / 1e9 / peak,
+               "peak_gbs": peak, "peak_source": peak_kind,
                "cpu_ms": cpu_s * 1e3, "cpu_pairs_per_s": npairs / cpu_s,
                "cpu": {"kind": "reference" if have_ref else "port",
                        "cores": cores if have_ref else 1},
                "speedup": cpu_s / gpu_s}
+        if len(grids) > 1:
+            row["grids_ms"] = {g: v[0] for g, v in grid_rows.items()}
+        if check:
+            # the bufs hold the last grid's build; every grid gives the same list
+            row["parity"] = _same_device(q, [bufs[c] for c in q], res)
+        del res
         if name.startswith("C5"):
             off = torch.empty(nat + 1, dtype=torch.int64, device=dev)
             ext.check(ext.lib.nbl_row_offsets(plan, ctypes.c_void_p(off.data_ptr()), sptr))
@@ -527,53 +644,82 @@ def _lj_line(out, dev, flush, reps, stream, sptr, plan, W, O, ext, have_ref, cpu
         "speedup": cpu_s / (gms * 1e-3)}
 
 
-def cpu_baseline(steps=2):
-    """The reference's CPU core on the same workload (rank 0, N = 1)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    from matscipy_neighbours import _workloads as W
+def _cpu_fn(O, cores):
+    """The reference's own core (oracle/_ref, OpenMP, `cores` threads) when it
+    was built, else the C restatement (one thread)."""
+    if O.ref_available():
+        O.ref_set_threads(cores)
+        return "reference", cores, O.ref_neighbour_list
+    return "port", 1, O.oracle_neighbour_list
+
+
+def workload_config(nat, reps, npairs, world):
+    """The `config` object of both arms' JSON lines (identical on purpose)."""
+    return dict(WORKLOAD, natoms=nat, reps=reps, npairs_per_step=npairs,
+                parallelism=f"replicas{world}",
+                l2="working set larger than L2 (2.5 GB of pairs written per step); "
+                   "the GPU arm also flushes L2 (256 MiB write) between steps")
+
+
+def cpu_baseline(steps=2, want=None):
+    """The reference's CPU core on the same workload (rank 0, N = 1), every
+    host thread, plus a one-thread row on a bounded sample (32^3 FCC cells,
+    1/8 of the workload) for context.  With `want` (a callable taking the
+    core's full "ijdDS" result) the last full result is handed over before it
+    is freed, for the parity check."""
+    O = _oracle()
+    W = _workloads()
     w = W.fcc_bulk(seed=0)
     cores = len(os.sched_getaffinity(0))
-    if O.ref_available():
-        kind = "reference"
-        O.ref_set_threads(cores)
-        fn = O.ref_neighbour_list
-    else:
-        kind, cores = "port", 1
-        fn = O.oracle_neighbour_list
+    kind, cores, fn = _cpu_fn(O, cores)
     fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])  # warm-up
     times, npairs = [], 0
-    for _ in range(steps):
+    for k in range(steps):
         t0 = time.perf_counter()
-        i = fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])[0]
+        res = fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])
         times.append(time.perf_counter() - t0)
-        npairs = len(i)
+        npairs = len(res[0])
+        if want is not None and k == steps - 1:
+            want(res)
+        del res
     med = statistics.median(times)
-    return {"value": npairs / med, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"full workload ({npairs} pairs), median of {steps} calls",
-            "seconds_per_call": med}
+    out = {"value": npairs / med, "unit": UNIT, "cores": cores, "kind": kind,
+           "sample": f"full workload ({npairs} pairs), median of {steps} calls",
+           "seconds_per_call": med}
+    if kind == "reference":
+        ws = W.fcc_bulk(seed=0, reps=32)
+        O.ref_set_threads(1)
+        fn("ijdDS", ws["cell"], ws["positions"], ws["cutoff"], ws["pbc"])
+        t1 = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            n1 = len(fn("ijdDS", ws["cell"], ws["positions"], ws["cutoff"], ws["pbc"])[0])
+            t1.append(time.perf_counter() - t0)
+        O.ref_set_threads(cores)
+        m1 = statistics.median(t1)
+        out["one_thread"] = {"value": n1 / m1, "unit": UNIT, "cores": 1, "kind": kind,
+                             "sample": f"32^3 FCC cells (131072 atoms, {n1} pairs), "
+                                       f"median of 3 calls",
+                             "seconds_per_call": m1}
+    return out
 
 
 def run_reference(args, rank):
-    """The reference's own CPU core, every host thread.  Each step is a bounded
-    sample of the workload: the same lattice, shear, jitter and cutoff at 32^3
-    unit cells (131,072 atoms, 1/8 of the benchmark size), so that K steps stay
-    within a few minutes; pairs/s is the rate the core sustains."""
+    """The reference's own CPU core (oracle/_ref: its neighbour_list.cc and
+    cell_list.cc compiled from source, OpenMP) on every host thread, on the
+    full benchmark workload: each step is one complete "ijdDS" build of the
+    1,048,576-atom sheared FCC bulk.  Nothing of the engine is loaded in this
+    process (the generators come from their own file).  Under torchrun only
+    rank 0 runs; the other ranks exit without work."""
     if rank != 0:
         return
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    from matscipy_neighbours import _workloads as W
-    w = W.fcc_bulk(seed=0, reps=32)
+    O = _oracle()
+    W = _workloads()
+    w = W.fcc_bulk(seed=0, reps=args.reps)
+    nat = w["positions"].shape[0]
     cores = len(os.sched_getaffinity(0))
-    if O.ref_available():
-        kind = "reference"
-        O.ref_set_threads(cores)
-        fn = O.ref_neighbour_list
-    else:
-        kind, cores = "port", 1
-        fn = O.oracle_neighbour_list
-    for _ in range(max(1, min(args.warmup, 3))):
+    kind, cores, fn = _cpu_fn(O, cores)
+    for _ in range(args.warmup):
         fn("ijdDS", w["cell"], w["positions"], w["cutoff"], w["pbc"])
     times, npairs = [], 0
     for _ in range(args.steps):
@@ -587,10 +733,10 @@ def run_reference(args, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism="host threads"),
+        "config": workload_config(nat, args.reps, npairs, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"1/8 of the workload per step: 32^3 FCC cells, "
-                                   f"131072 atoms, {npairs} pairs"},
+                         "sample": f"the full workload every step ({nat} atoms, "
+                                   f"{npairs} pairs), host wall clock per call"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -603,6 +749,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the bit-for-bit comparisons with the CPU checker")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
@@ -630,7 +778,7 @@ def main():
 
     import matscipy_neighbours as m
     from matscipy_neighbours import _matscipy_neighbours as ext
-    from matscipy_neighbours import _workloads as W
+    W = _workloads()
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -772,10 +920,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, natoms=nat, reps=args.reps, npairs_per_step=npairs,
-                       parallelism=f"replicas{world}",
-                       l2="flushed between steps (256 MiB write, outside the events)",
-                       precision="fp32 filter + fp64 guard-band recheck"),
+        "config": workload_config(nat, args.reps, npairs, world),
+        "precision": "fp32 filter + fp64 guard-band recheck",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": _traffic_per_launch(npairs, nat),
@@ -795,12 +941,34 @@ def main():
         "stage_ms": {"count_phase": statistics.mean(a - b for a, b in zip(step_ms, fill_ms)),
                      "fill": statistics.mean(fill_ms)},
     }
+    parity = {}
     if not args.no_batched:
-        out["batched"] = batched_bench(min(args.steps, 20), args.warmup, dev, rank)
+        out["batched"] = batched_bench(min(args.steps, 20), args.warmup, dev, rank,
+                                       check=world == 1 and not args.no_parity)
+        if "parity" in out["batched"]:
+            parity["C4"] = out["batched"]["parity"]
     if world == 1 and not args.no_configs:
-        out["configs"] = configs_bench(dev, flush)
+        out["configs"] = configs_bench(dev, flush, check=not args.no_parity)
+        for name, key in (("C1_plain_small", "C1"), ("C3_sparse_slab", "C3"),
+                          ("C5_diff_lattice", "C5")):
+            if "parity" in out["configs"].get(name, {}):
+                parity[key] = out["configs"][name]["parity"]
     if world == 1 and not args.no_cpu_baseline and args.reps == 64:
-        out["cpu_baseline"] = cpu_baseline()
+        want = None
+        if not args.no_parity:
+            # the headline build once more (FP32 filter), outside any timing,
+            # compared with the reference core's last full result
+            timed_steps(req, 1)
+            ext.check(ext.lib.nbl_check(plan, sptr))
+
+            def want(res):
+                parity["C2"] = _same_device("ijdDS", [outs[q] for q in "ijdDS"], res)
+        out["cpu_baseline"] = cpu_baseline(want=want)
+    if parity:
+        out["parity"] = parity
+        out["parity_checker"] = ("oracle/_ref (the reference's own CPU core, compiled from its "
+                                 "sources)" if _oracle().ref_available()
+                                 else "oracle (C restatement of the reference CPU path)")
     print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()

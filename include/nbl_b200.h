@@ -377,10 +377,12 @@ NBL_API nbl_status nbl_triplet_list(int64_t nfirst, const int32_t *first_i,
    until exit; at most NBL_NOALLOC_MAX_ATOMS atoms.  Inputs as in nbl_request
    (positions device or host); `out` holds caller-allocated DEVICE buffers of
    `capacity` pairs.  Sets *npairs and returns NBL_ERROR_CAPACITY (writing
-   nothing) when npairs > capacity.  Synchronises `stream`.  Calls overlapping
-   on the GPU race on the shared scratch: serialise them.  The first call on a
-   device resolves the scratch address (device must be current) and should
-   come before any stream capture. */
+   nothing) when npairs > capacity.  Synchronises `stream`: on return the
+   outputs are written and the scratch is free again.  Calls overlapping on
+   the GPU race on the shared scratch: serialise them.  The first call on a
+   device resolves the scratch address (device must be current), caches it for
+   the life of the process (one primary context per device is assumed: not
+   valid across cudaDeviceReset) and should come before any stream capture. */
 #define NBL_NOALLOC_MAX_ATOMS 32768
 NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
                                               const nbl_outputs *out,

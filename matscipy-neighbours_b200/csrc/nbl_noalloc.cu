@@ -23,8 +23,14 @@
 //     overlap on the GPU (different streams, or different host threads) race
 //     on it and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (that device current) and caches it; make that
-//     first call before starting any stream capture.
+//     cudaGetSymbolAddress (that device current) and caches it per device
+//     ordinal for the life of the process; make that first call before
+//     starting any stream capture.  The cache assumes the process keeps one
+//     (primary) context per device: after cudaDeviceReset, or under a context
+//     of its own on that device, the cached address is stale;
+//   * the call returns after the fill has finished (it synchronises `stream`
+//     twice: for the pair count and at the end) and reports errors the device
+//     flagged in either pass.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -120,8 +126,11 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "nbl_neighbour_list_noalloc: make device %d current first", dev);
 
-    // Plan the system on the host exactly as nbl_count does; the grid falls
-    // back to the hashed table when a dense table would not fit.
+    // Plan the system on the host as nbl_count does, with one difference: a
+    // dense or Morton table of more than 2^18 cells (whether the caller asked
+    // for it or the automatic rule chose it) is replaced by the hashed table,
+    // whose size follows the atom count, so that it fits the static scratch.
+    // Every grid gives the same output.
     nbl_request r = *req;
     Batch b;
     nbl_status st = batch_from_request(&r, b);
@@ -318,6 +327,17 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.shift = out->shift;
     ta.capacity = capacity;
     NA_CUDA(launch_traverse(kModeFill, b.fp32, kind, ta, fill_grid, s), "fill pass");
+    // The call returns only when the fill has finished with the shared scratch,
+    // and reports what the device flagged during it.
+    NA_CUDA(cudaMemcpyAsync(flags, small, sizeof(flags), cudaMemcpyDeviceToHost, s),
+            "read flags");
+    NA_CUDA(cudaStreamSynchronize(s), "fill pass");
+    if (flags[1] & kErrCapacity)
+        return set_error(NBL_ERROR_CAPACITY,
+                         "nbl_neighbour_list_noalloc: a pair fell outside the output "
+                         "capacity %lld", (long long)capacity);
+    if (flags[1] & kErrInternal)
+        return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded in fill pass");
 #undef NA_CUDA
     return NBL_SUCCESS;
 }

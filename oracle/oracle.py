@@ -65,13 +65,20 @@ _lib = None
 _ref = None
 
 
+def reference_src():
+    """The reference's src/libneighbours directory: NBL_REFERENCE_SRC, else that
+    of a checkout of the reference beside this repository (../reference)."""
+    return pathlib.Path(os.environ.get(
+        "NBL_REFERENCE_SRC", HERE.parent.parent / "reference" / "src" / "libneighbours"))
+
+
 def build():
     """Compile the C restatement (and the reference core when its sources are
     present).  Cheap and idempotent."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if os.path.isdir(os.environ.get("NBL_REFERENCE_SRC",
-                                    "/root/reference/src/libneighbours")):
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    src = reference_src()
+    if src.is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_SRC={src}"], check=True)
 
 
 def _load():
