@@ -389,6 +389,23 @@ NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
                                               int64_t capacity, int64_t *npairs,
                                               void *stream);
 
+/* Test hooks: failures made on the host, so that the error paths can be
+   exercised without faulting a GPU.  No counterpart in the reference, whose
+   device errors abort the process (src/libneighbours/device.hh:68-74).
+     NBL_INJECT_ALLOC_FAILURES  the next `value` growths of a plan's device
+                                workspace fail as if the device were out of
+                                memory (nbl_count returns
+                                NBL_ERROR_OUT_OF_MEMORY and keeps nothing);
+     NBL_INJECT_HASH_CAPACITY   hashed grids get `value` slots (rounded up to a
+                                power of two) instead of 2N+1 rounded up; 0
+                                restores the default.  With fewer slots than
+                                occupied cells the bounded probe gives up and
+                                the count returns NBL_ERROR_INTERNAL.
+   Process-wide; not for production use. */
+#define NBL_INJECT_ALLOC_FAILURES 1
+#define NBL_INJECT_HASH_CAPACITY 2
+NBL_API nbl_status nbl_debug_inject(int what, int64_t value);
+
 /* Last error message of the calling thread ("" if none). */
 NBL_API const char *nbl_last_error(void);
 

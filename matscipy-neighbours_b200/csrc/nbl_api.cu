@@ -7,6 +7,7 @@
 // compiled without FP contraction, so the device sees the same doubles the
 // reference CPU core computes.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -168,11 +169,22 @@ void Workspace::release() {
     out_bytes = 0;
 }
 
+// Host-side failure injection (nbl_debug_inject): workspace growths that are
+// made to fail, and a forced hashed-table size.
+static std::atomic<int64_t> g_inject_alloc_failures{0};
+static std::atomic<int64_t> g_inject_hash_capacity{0};
+
 static nbl_status ensure(void *&ptr, size_t &have, size_t need, const char *what) {
     if (need <= have) return NBL_SUCCESS;
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     have = 0;
+    for (int64_t n = g_inject_alloc_failures.load(); n > 0;
+         n = g_inject_alloc_failures.load()) {
+        if (g_inject_alloc_failures.compare_exchange_weak(n, n - 1))
+            return set_error(NBL_ERROR_OUT_OF_MEMORY,
+                             "%s: cannot allocate %zu bytes (injected failure)", what, need);
+    }
     size_t grow = need + need / 4;
     cudaError_t e = cudaMalloc(&ptr, grow);
     if (e != cudaSuccess) {
@@ -258,7 +270,11 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_items = L.add(sizeof(int2) * std::max<int64_t>(N, 1));
     size_t o_ljp = L.add(sizeof(double) * (size_t)(std::max<int64_t>(N, 1) + N / 1024 + 64));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
-    if (st != NBL_SUCCESS) return st;
+    if (st != NBL_SUCCESS) {
+        B = Bufs();  // nothing may point into the released block
+        p.have_count = false;
+        return st;
+    }
     char *base = static_cast<char *>(p.ws.base);
     auto at = [&](size_t off) { return static_cast<void *>(base + off); };
     B.pos = b.pos_on_device ? const_cast<double *>(b.positions) : (double *)at(o_pos);
@@ -342,7 +358,8 @@ nbl_status finish_batch(Batch &b, int grid_req) {
     }
     if (b.grid == kGridHashed) {
         int64_t cap = 1;
-        while (cap < 2 * std::max<int64_t>(b.natoms, 1) + 1) cap <<= 1;
+        const int64_t forced = g_inject_hash_capacity.load();
+        while (cap < (forced > 0 ? forced : 2 * std::max<int64_t>(b.natoms, 1) + 1)) cap <<= 1;
         b.table_size = cap;
         b.key_bits = bits_for((uint64_t)(cap - 1));
     } else {
@@ -449,6 +466,7 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
 // batch whose inputs are resident: no host synchronisation, no allocation,
 // so it can be captured in a CUDA graph.
 nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
+    StageRange whole("nbl.count_phase");
     Bufs &B = p.bufs;
     const int64_t N = b.natoms;
     const int nsys = (int)b.sys.size();
@@ -474,12 +492,18 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ba.hkey = B.hkey;
     ba.hmask = (unsigned long long)(b.table_size - 1);
     ba.err = err;
-    NBL_CUDA(launch_bin(ba, st), "k_bin");
+    {
+        StageRange r("nbl.bin");
+        NBL_CUDA(launch_bin(ba, st), "k_bin");
+    }
 
     bool in_alt = false;
-    NBL_CUDA(radix_sort_pairs(B.keys, B.vals, B.keys2, B.vals2, N, b.key_bits, B.hist,
-                              B.hist_scan, B.scan32, st, &in_alt),
-             "radix sort");
+    {
+        StageRange r("nbl.sort");
+        NBL_CUDA(radix_sort_pairs(B.keys, B.vals, B.keys2, B.vals2, N, b.key_bits, B.hist,
+                                  B.hist_scan, B.scan32, st, &in_alt),
+                 "radix sort");
+    }
     const uint32_t *skeys = in_alt ? B.keys2 : B.keys;
     const int32_t *svals = in_alt ? B.vals2 : B.vals;
 
@@ -501,10 +525,14 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ga.amax = B.amax;
     ga.home = B.home;
     ga.n_home = n_home;
-    NBL_CUDA(launch_gather(ga, st), "k_gather");
-    NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms, st),
-             "k_tiles");
-    NBL_CUDA(launch_visit(B.sys, nsys, B.visit, st), "k_visit");
+    {
+        StageRange r("nbl.gather");
+        NBL_CUDA(launch_gather(ga, st), "k_gather");
+        NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms,
+                              st),
+                 "k_tiles");
+        NBL_CUDA(launch_visit(B.sys, nsys, B.visit, st), "k_visit");
+    }
 
     TraverseArgs &ta = p.targs;
     std::memset(&ta, 0, sizeof(ta));
@@ -540,10 +568,16 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     p.trav_grid = traverse_grid(p, N, p.count_mult, kModeCount, b.fp32, p.batch_kind,
                                 p.count_group, false);
     p.fill_grid = traverse_grid(p, N, p.fill_mult, kModeFill, b.fp32, p.batch_kind, 4, false);
-    NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
-                             p.count_group),
-             "count pass");
-    NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
+    {
+        StageRange r("nbl.count");
+        NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
+                                 p.count_group),
+                 "count pass");
+    }
+    {
+        StageRange r("nbl.scan");
+        NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
+    }
     return NBL_SUCCESS;
 }
 
@@ -589,6 +623,7 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     ta.shift = o.shift;
     ta.capacity = capacity;
     if (!(o.first || o.second || o.distvec || o.absdist || o.shift)) return NBL_SUCCESS;
+    StageRange r("nbl.fill");
     NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st),
              "fill pass");
     return NBL_SUCCESS;
@@ -761,6 +796,21 @@ nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi) {
                          (long long)lo, (long long)hi);
     plan->p.i_lo = lo;
     plan->p.i_hi = hi;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_debug_inject(int what, int64_t value) {
+    clear_error();
+    if (value < 0) return set_error(NBL_ERROR_INVALID_ARGUMENT, "negative injection value");
+    if (what == NBL_INJECT_ALLOC_FAILURES) {
+        g_inject_alloc_failures.store(value);
+    } else if (what == NBL_INJECT_HASH_CAPACITY) {
+        if (value > (int64_t(1) << 40))
+            return set_error(NBL_ERROR_INVALID_ARGUMENT, "hash capacity too large");
+        g_inject_hash_capacity.store(value);
+    } else {
+        return set_error(NBL_ERROR_INVALID_ARGUMENT, "unknown injection %d", what);
+    }
     return NBL_SUCCESS;
 }
 

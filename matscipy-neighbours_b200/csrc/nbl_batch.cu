@@ -530,12 +530,13 @@ NBL_API nbl_status nbl_batch_finish(nbl_batch *bt, void *stream, int64_t *npairs
     if (flags[1] & kErrRange)
         return set_error(NBL_ERROR_RANGE,
                          "positions must be finite and within 2^29 cells of the box");
+    // an internal bound makes the pair count meaningless: report it first
+    if (flags[1] & kErrInternal)
+        return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded");
     if (*npairs > bt->capacity || (flags[1] & kErrCapacity))
         return set_error(NBL_ERROR_CAPACITY,
                          "%lld pairs exceed the batch capacity %lld; set up again with a "
                          "larger capacity", (long long)*npairs, (long long)bt->capacity);
-    if (flags[1] & kErrInternal)
-        return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded");
     return NBL_SUCCESS;
 }
 

@@ -819,58 +819,67 @@ k_count(TraverseArgs a) {
                                 ny[h] = make_float2(-pg[2 * h].y, -pg[2 * h + 1].y);
                                 nz[h] = make_float2(-pg[2 * h].z, -pg[2 * h + 1].z);
                             }
-                            for (int ch = 0; ch < nck; ch++) {
-                                const int k = ch * 32 + lane;
-                                const float4 cv = sm.cand[k];
-                                unsigned m[GROUP];
-                                bool amb_any = false, amb[GROUP];
-                                float r2g[GROUP];
-                                const float2 cx = make_float2(cv.x, cv.x);
-                                const float2 cy = make_float2(cv.y, cv.y);
-                                const float2 cz = make_float2(cv.z, cv.z);
+                            // blocks of up to 32 chunks: lane L keeps chunk cb + L's hit
+                            // word of each atom; the block's counts and its pool words
+                            // are taken once at its end
+                            for (int cb = 0; cb < nck; cb += 32) {
+                                const int ce = min(nck, cb + 32);
 #pragma unroll
-                                for (int h = 0; h < kHalf; h++) {
-                                    const float2 dx = __fadd2_rn(cx, nx[h]);
-                                    const float2 dy = __fadd2_rn(cy, ny[h]);
-                                    const float2 dz = __fadd2_rn(cz, nz[h]);
-                                    const float2 r2 =
-                                        __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                    r2g[2 * h] = r2.x;
-                                    r2g[2 * h + 1] = r2.y;
-                                }
+                                for (int g = 0; g < GROUP; g++) mw[g] = 0u;
+                                for (int ch = cb; ch < ce; ch++) {
+                                    const int k = ch * 32 + lane;
+                                    const float4 cv = sm.cand[k];
+                                    unsigned m[GROUP];
+                                    bool amb_any = false, amb[GROUP];
+                                    float r2g[GROUP];
+                                    const float2 cx = make_float2(cv.x, cv.x);
+                                    const float2 cy = make_float2(cv.y, cv.y);
+                                    const float2 cz = make_float2(cv.z, cv.z);
 #pragma unroll
-                                for (int g = 0; g < GROUP; g++) {
-                                    const float r2 = r2g[g];
-                                    float lo, hi;
-                                    thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
-                                    const bool notself = k != ks[g];
-                                    m[g] = __ballot_sync(full, (r2 < lo) && notself);
-                                    amb[g] = !(r2 < lo) && (r2 < hi) && notself;
-                                    amb_any |= amb[g];
-                                }
-                                if (__any_sync(full, amb_any)) {
-#pragma unroll
-                                    for (int g = 0; g < GROUP; g++) {
-                                        bool h2 = false;
-                                        if (amb[g])
-                                            h2 = resolve_exact<KIND>(sm.sg, a, H, nseg, kb + k,
-                                                                     sm.isi[g0 + g], pg[g].w);
-                                        m[g] |= __ballot_sync(full, h2);
+                                    for (int h = 0; h < kHalf; h++) {
+                                        const float2 dx = __fadd2_rn(cx, nx[h]);
+                                        const float2 dy = __fadd2_rn(cy, ny[h]);
+                                        const float2 dz = __fadd2_rn(cz, nz[h]);
+                                        const float2 r2 = __ffma2_rn(
+                                            dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                        r2g[2 * h] = r2.x;
+                                        r2g[2 * h + 1] = r2.y;
                                     }
-                                }
-                                const bool mine = lane == (ch & 31);
-#pragma unroll
-                                for (int g = 0; g < GROUP; g++) {
-                                    cnt[g] += __popc(m[g]);
-                                    mw[g] = mine ? m[g] : mw[g];
-                                }
-                                if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
-                                    const long long w0 = mbase + (kb >> 5) + (ch & ~31) + lane;
 #pragma unroll
                                     for (int g = 0; g < GROUP; g++) {
-                                        if (g0 + g < ni && lane <= (ch & 31))
-                                            a.mask_pool[w0 + (long long)(g0 + g) *
-                                                                 nchunks_all] = mw[g];
+                                        const float r2 = r2g[g];
+                                        float lo, hi;
+                                        thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
+                                        const bool notself = k != ks[g];
+                                        m[g] = __ballot_sync(full, (r2 < lo) && notself);
+                                        amb[g] = !(r2 < lo) && (r2 < hi) && notself;
+                                        amb_any |= amb[g];
+                                    }
+                                    if (__any_sync(full, amb_any)) {
+#pragma unroll
+                                        for (int g = 0; g < GROUP; g++) {
+                                            bool h2 = false;
+                                            if (amb[g])
+                                                h2 = resolve_exact<KIND>(sm.sg, a, H, nseg,
+                                                                         kb + k, sm.isi[g0 + g],
+                                                                         pg[g].w);
+                                            m[g] |= __ballot_sync(full, h2);
+                                        }
+                                    }
+                                    const bool mine = lane == ch - cb;
+#pragma unroll
+                                    for (int g = 0; g < GROUP; g++) mw[g] = mine ? m[g] : mw[g];
+                                }
+#pragma unroll
+                                for (int g = 0; g < GROUP; g++)
+                                    cnt[g] += (int)__reduce_add_sync(full, (unsigned)__popc(mw[g]));
+                                if (mbase >= 0 && lane < ce - cb) {
+                                    const long long w0 = mbase + (kb >> 5) + cb + lane;
+#pragma unroll
+                                    for (int g = 0; g < GROUP; g++) {
+                                        if (g0 + g < ni)
+                                            a.mask_pool[w0 + (long long)(g0 + g) * nchunks_all] =
+                                                mw[g];
                                     }
                                 }
                             }
