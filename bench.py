@@ -222,7 +222,7 @@ def batched_bench(steps, warmup, dev, rank=0, check=False):
     b64 = NeighbourListBatch(systems, precision="fp64", graph=True, autotune=True,
                              device=dev.index)
     fp64_ms = _time_batch(b64, steps, warmup)
-    cfg64 = b64.config()
+    lc64 = b64.launch_config()
     b64.close()
     b = NeighbourListBatch(systems, precision="fp32", graph=True, autotune=True,
                            device=dev.index)
@@ -242,8 +242,7 @@ def batched_bench(steps, warmup, dev, rank=0, check=False):
                 parity = False
                 break
         del res
-    cfg = b.config()
-    tickets = b.tickets()
+    lc = b.launch_config()
     positions = b.positions
     offs = b.atom_offsets
     b.close()
@@ -300,15 +299,14 @@ def batched_bench(steps, warmup, dev, rank=0, check=False):
            "atoms": int(offs[-1]), "npairs": int(npairs),
            "batched_fp32_graph": {"value": npairs / batched_s, "unit": UNIT,
                                   "ms_per_step": batched_ms,
-                                  "launch_config": {"count_ctas_per_sm": cfg[0],
-                                                    "count_atoms_per_pass": cfg[1],
-                                                    "fill_ctas_per_sm": cfg[2],
-                                                    "count_item_tickets": tickets[0],
-                                                    "fill_item_tickets": tickets[1]}},
+                                  "stage_ms_at_tuning": {"count_phase": lc["tuned_count_ms"],
+                                                         "fill": lc["tuned_fill_ms"]},
+                                  "launch_config": lc},
            "batched_fp64_graph": {"value": npairs / (fp64_ms * 1e-3), "unit": UNIT,
                                   "ms_per_step": fp64_ms,
-                                  "launch_config": {"count_ctas_per_sm": cfg64[0],
-                                                    "fill_ctas_per_sm": cfg64[2]}},
+                                  "stage_ms_at_tuning": {"count_phase": lc64["tuned_count_ms"],
+                                                         "fill": lc64["tuned_fill_ms"]},
+                                  "launch_config": lc64},
            "plain_fp64_per_system": {"value": npairs / plain_s, "unit": UNIT,
                                      "ms_per_step": plain_s * 1e3,
                                      "note": "one nbl_count + nbl_fill per system, host "

@@ -152,6 +152,37 @@ NBL_API nbl_status nbl_set_atom_range(nbl_plan *plan, int64_t lo, int64_t hi);
 NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, int count_group,
                                        int fill_ctas_per_sm);
 
+/* The full launch configuration of the pair passes (what the batch
+   autotuner chooses; a single call uses the defaults unless set here).  Every
+   value gives bit-identical output.  Zero fields mean the default.
+     count_ctas_per_sm, fill_ctas_per_sm  grid of each pass (0: two waves of
+                                          its resident CTAs), <= 64
+     count_strided, fill_strided          work items by a fixed warp stride
+                                          (1) instead of by atomic ticket (0)
+     count_warps, fill_warps              block size: 2, 4 or 8 warps
+                                          (64, 128 or 256 threads; default 4)
+     count_group                          atoms per FP32 sweep: 2 or 4 (4)
+     count_large_staging                  candidates staged per count warp:
+                                          0 = 384 (FP32) / 192 (FP64),
+                                          1 = 768 / 384
+     atoms_per_item                       cell-occupancy tile: atoms of one
+                                          cell per work item, 1..32 (32)
+   No reference counterpart (the reference has no tuner). */
+typedef struct nbl_launch_config {
+    int count_ctas_per_sm;
+    int fill_ctas_per_sm;
+    int count_strided;
+    int fill_strided;
+    int count_warps;
+    int fill_warps;
+    int count_group;
+    int count_large_staging;
+    int atoms_per_item;
+} nbl_launch_config;
+
+NBL_API nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *cfg);
+NBL_API nbl_status nbl_plan_get_launch_config(nbl_plan *plan, nbl_launch_config *cfg);
+
 /* Count phase: bins the atoms, counts every atom's neighbours and scans the
    counts into row offsets.  Host positions are copied in on `stream`.
    Synchronises `stream` to return the pair count. */
@@ -277,6 +308,11 @@ NBL_API nbl_status nbl_batch_get_config(nbl_batch *batch, int *count_mult,
    or by a fixed warp stride (0), as the autotuner chose. */
 NBL_API nbl_status nbl_batch_get_tickets(nbl_batch *batch, int *count_tickets,
                                          int *fill_tickets);
+/* Everything the autotuner chose (nbl_launch_config above), and the median
+   device times (ms) of the count phase and of the fill with that choice, as
+   the autotuner measured them (0 when it did not run). */
+NBL_API nbl_status nbl_batch_get_launch_config(nbl_batch *batch, nbl_launch_config *cfg,
+                                               float *count_ms, float *fill_ms);
 
 /* ---- backward: gradients through the pair list -------------------------
    (Build-only form with no reference counterpart.)  For a fixed pair list of

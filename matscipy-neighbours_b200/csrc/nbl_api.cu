@@ -380,9 +380,9 @@ nbl_status finish_batch(Batch &b, int grid_req) {
 // items in a fixed stride, so a grid that is not a whole number of waves
 // leaves its last partial wave running alone.
 static int traverse_grid(const Plan &p, int64_t natoms, int mult, int mode, bool fp32,
-                         int kind, int group, bool lj) {
+                         int kind, const TravShape &shape, bool lj) {
     if (mult <= 0)
-        mult = kAutoWaves * std::max(1, traverse_blocks_per_sm(mode, fp32, kind, group, lj));
+        mult = kAutoWaves * std::max(1, traverse_blocks_per_sm(mode, fp32, kind, shape, lj));
     const int64_t items = std::max<int64_t>((natoms + 3) / 4, 1);
     return (int)std::min<int64_t>((int64_t)p.num_sms * mult, items);
 }
@@ -529,7 +529,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
         StageRange r("nbl.gather");
         NBL_CUDA(launch_gather(ga, st), "k_gather");
         NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms,
-                              st),
+                              p.itile, st),
                  "k_tiles");
         NBL_CUDA(launch_visit(B.sys, nsys, B.visit, st), "k_visit");
     }
@@ -562,16 +562,18 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.err = err;
     ta.i_lo = p.i_lo;
     ta.i_hi = p.i_hi;
+    ta.itile = p.itile;
     if (p.i_lo > 0 || p.i_hi < N)
         NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
     p.trav_grid = traverse_grid(p, N, p.count_mult, kModeCount, b.fp32, p.batch_kind,
-                                p.count_group, false);
-    p.fill_grid = traverse_grid(p, N, p.fill_mult, kModeFill, b.fp32, p.batch_kind, 4, false);
+                                p.count_shape, false);
+    p.fill_grid = traverse_grid(p, N, p.fill_mult, kModeFill, b.fp32, p.batch_kind,
+                                p.fill_shape, false);
     {
         StageRange r("nbl.count");
         NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
-                                 p.count_group),
+                                 p.count_shape),
                  "count pass");
     }
     {
@@ -624,7 +626,8 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     ta.capacity = capacity;
     if (!(o.first || o.second || o.distvec || o.absdist || o.shift)) return NBL_SUCCESS;
     StageRange r("nbl.fill");
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st),
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st,
+                             p.fill_shape),
              "fill pass");
     return NBL_SUCCESS;
 }
@@ -643,6 +646,19 @@ nbl_status read_flags(Plan &p, cudaStream_t st) {
     if (flags[1] & kErrInternal)
         return set_error(NBL_ERROR_INTERNAL, "device-side bound exceeded");
     return NBL_SUCCESS;
+}
+
+// The plan's launch configuration in C-ABI form.
+void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
+    cfg->count_ctas_per_sm = p.count_mult;
+    cfg->fill_ctas_per_sm = p.fill_mult;
+    cfg->count_strided = p.count_tickets ? 0 : 1;
+    cfg->fill_strided = p.fill_tickets ? 0 : 1;
+    cfg->count_warps = p.count_shape.warps;
+    cfg->fill_warps = p.fill_shape.warps;
+    cfg->count_group = p.count_shape.group;
+    cfg->count_large_staging = p.count_shape.cand;
+    cfg->atoms_per_item = p.itile;
 }
 
 // Request -> one-system batch.
@@ -824,7 +840,39 @@ nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, int count_
                          "launch: CTAs per SM in [0, 64], count group 0, 2 or 4");
     plan->p.count_mult = count_ctas_per_sm;
     plan->p.fill_mult = fill_ctas_per_sm;
-    plan->p.count_group = count_group == 0 ? 4 : count_group;
+    plan->p.count_shape.group = count_group == 0 ? 4 : count_group;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *cfg) {
+    clear_error();
+    if (!plan || !cfg) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    TravShape cs, fs;
+    cs.warps = cfg->count_warps == 0 ? 4 : cfg->count_warps;
+    cs.cand = cfg->count_large_staging;
+    cs.group = cfg->count_group == 0 ? 4 : cfg->count_group;
+    fs.warps = cfg->fill_warps == 0 ? 4 : cfg->fill_warps;
+    const int itile = cfg->atoms_per_item == 0 ? 32 : cfg->atoms_per_item;
+    if (cfg->count_ctas_per_sm < 0 || cfg->count_ctas_per_sm > 64 || cfg->fill_ctas_per_sm < 0 ||
+        cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 ||
+        !traverse_shape_ok(kModeCount, true, cs) || !traverse_shape_ok(kModeFill, true, fs))
+        return set_error(NBL_ERROR_INVALID_ARGUMENT,
+                         "launch config: CTAs per SM in [0, 64], warps 2, 4 or 8, count group "
+                         "2 or 4, large candidate staging 0 or 1, atoms per item in [1, 32]");
+    plan->p.count_mult = cfg->count_ctas_per_sm;
+    plan->p.fill_mult = cfg->fill_ctas_per_sm;
+    plan->p.count_tickets = cfg->count_strided == 0;
+    plan->p.fill_tickets = cfg->fill_strided == 0;
+    plan->p.count_shape = cs;
+    plan->p.fill_shape = fs;
+    plan->p.itile = itile;
+    return NBL_SUCCESS;
+}
+
+nbl_status nbl_plan_get_launch_config(nbl_plan *plan, nbl_launch_config *cfg) {
+    clear_error();
+    if (!plan || !cfg) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    launch_config_of(plan->p, cfg);
     return NBL_SUCCESS;
 }
 
@@ -928,7 +976,8 @@ nbl_status nbl_fill_matrix(nbl_plan *plan, int32_t max_neighbours, int32_t *idx,
     ta.mat_count = count;
     ta.mat_overflow = p.bufs.small + 2;
     ta.capacity = 0;
-    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st),
+    NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, p.fill_grid, st,
+                             p.fill_shape),
              "matrix fill");
     NBL_CUDA(cudaMemcpyAsync(p.host_small + 2, p.bufs.small + 2, sizeof(int),
                              cudaMemcpyDeviceToHost, st), "read overflow");
@@ -975,7 +1024,7 @@ nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
     ta.lj_eps24 = 24.0 * epsilon;
     ta.lj_sig2 = sigma * sigma;
     const int grid = traverse_grid(p, b.natoms, p.fill_mult, kModeFill, p.batch_fp32,
-                                   p.batch_kind, 4, true);
+                                   p.batch_kind, TravShape(), true);
     NBL_CUDA(launch_traverse(kModeFill, p.batch_fp32, p.batch_kind, ta, grid, cs),
              "force pass");
     NBL_CUDA(launch_lj_energy(p.bufs.lj_part, b.natoms, p.bufs.lj_part + b.natoms, energy,

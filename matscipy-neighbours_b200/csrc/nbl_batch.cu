@@ -10,11 +10,17 @@
 // writes at most `capacity` pairs and flags an overflow that nbl_batch_finish
 // reports (with the true count, so the caller can set up a larger batch).
 //
-// Autotuner: the pair passes' launch configuration -- CTAs per SM of the count
-// and fill kernels (1, 2 or 4 waves of their resident CTAs), work items by
-// atomic ticket or by fixed stride in each, and how many atoms the FP32 count
-// sweeps per pass over a candidate tile -- is timed on the batch itself at
-// set-up and the fastest choice is cached per (SM count, cutoff kind,
+// Autotuner: the pair passes' launch configuration is timed on the batch
+// itself at set-up, each candidate configuration as the median of five runs:
+//   * atoms per work item (the cell-occupancy tile): 32 or 16;
+//   * count pass: block size (2, 4 or 8 warps), candidates staged per warp
+//     (384 or 768 FP32 positions; 192 or 384 FP64), atoms per FP32 sweep
+//     (2 or 4), then its grid (1, 2 or 4 waves of its resident CTAs) and
+//     work items by atomic ticket or by fixed stride;
+//   * fill pass: block size, then grid and tickets.
+// The search is staged (shape first at two waves with tickets, then the grid
+// for the best shape) for each tile size, and the tile size with the lower
+// count + fill time wins.  The choice is cached per (SM count, cutoff kind,
 // precision, atoms-per-cell bucket, visited-cells bucket), in memory and, when
 // NBL_TUNE_CACHE names a file, on disk.
 #include <algorithm>
@@ -48,7 +54,9 @@ __global__ void k_sys_offsets(const int64_t *__restrict__ offsets,
 }
 
 struct TuneChoice {
-    int count_mult, count_group, fill_mult, count_tickets, fill_tickets;
+    int count_mult = 0, count_group = 4, fill_mult = 0, count_tickets = 1, fill_tickets = 1;
+    int count_warps = 4, count_cand = 0, fill_warps = 4, itile = 32;
+    float count_ms = 0.f, fill_ms = 0.f;
 };
 
 std::mutex g_tune_mutex;
@@ -64,8 +72,10 @@ void tune_load_locked() {
     if (!f) return;
     char key[256];
     TuneChoice c;
-    while (std::fscanf(f, "%255s %d %d %d %d %d", key, &c.count_mult, &c.count_group,
-                       &c.fill_mult, &c.count_tickets, &c.fill_tickets) == 6)
+    while (std::fscanf(f, "%255s %d %d %d %d %d %d %d %d %d %f %f", key, &c.count_mult,
+                       &c.count_group, &c.fill_mult, &c.count_tickets, &c.fill_tickets,
+                       &c.count_warps, &c.count_cand, &c.fill_warps, &c.itile, &c.count_ms,
+                       &c.fill_ms) == 12)
         g_tune_cache[key] = c;
     std::fclose(f);
 }
@@ -76,8 +86,9 @@ void tune_store_locked(const std::string &key, const TuneChoice &c) {
     if (!path) return;
     FILE *f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d %d %d\n", key.c_str(), c.count_mult, c.count_group,
-                 c.fill_mult, c.count_tickets, c.fill_tickets);
+    std::fprintf(f, "%s %d %d %d %d %d %d %d %d %d %.6f %.6f\n", key.c_str(), c.count_mult,
+                 c.count_group, c.fill_mult, c.count_tickets, c.fill_tickets, c.count_warps,
+                 c.count_cand, c.fill_warps, c.itile, c.count_ms, c.fill_ms);
     std::fclose(f);
 }
 
@@ -113,6 +124,8 @@ struct nbl_batch {
     cudaGraphExec_t exec = nullptr;
     bool ready = false;
     std::string tune_key;
+    float tuned_count_ms = 0.f;
+    float tuned_fill_ms = 0.f;
 };
 
 namespace {
@@ -197,35 +210,167 @@ nbl_status batch_plan(const nbl_batch_request *req, Batch &b) {
     return finish_batch(b, req->grid);
 }
 
-// Time the count pass for the current launch configuration (ms).
+constexpr int kTuneRuns = 5;
+
+float median_ms(std::vector<float> &v) {
+    std::sort(v.begin(), v.end());
+    return v.empty() ? 1e30f : v[v.size() / 2];
+}
+
+// Median device time (ms) of kTuneRuns count phases with the current launch
+// configuration; 1e30 if a launch fails.
 float time_count(nbl_batch *bt, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
-    float best = 1e30f;
-    for (int r = 0; r < 2; r++) {
+    std::vector<float> ms;
+    for (int r = 0; r < kTuneRuns; r++) {
         cudaEventRecord(e0, st);
         if (enqueue_count(bt->p, bt->b, st) != NBL_SUCCESS) return 1e30f;
         cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        best = std::min(best, ms);
+        if (cudaEventSynchronize(e1) != cudaSuccess) return 1e30f;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms.push_back(t);
     }
-    return best;
+    return median_ms(ms);
 }
 
 float time_fill(nbl_batch *bt, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
-    float best = 1e30f;
+    std::vector<float> ms;
     nbl_outputs o{bt->outs.first, bt->outs.second, bt->outs.distvec, bt->outs.absdist,
                   bt->outs.shift};
-    for (int r = 0; r < 2; r++) {
+    for (int r = 0; r < kTuneRuns; r++) {
         cudaEventRecord(e0, st);
         if (run_fill(bt->p, o, bt->capacity, st) != NBL_SUCCESS) return 1e30f;
         cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        best = std::min(best, ms);
+        if (cudaEventSynchronize(e1) != cudaSuccess) return 1e30f;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms.push_back(t);
     }
-    return best;
+    return median_ms(ms);
+}
+
+void apply_choice(Plan &p, const TuneChoice &c) {
+    p.count_mult = c.count_mult;
+    p.fill_mult = c.fill_mult;
+    p.count_tickets = c.count_tickets != 0;
+    p.fill_tickets = c.fill_tickets != 0;
+    p.count_shape.warps = c.count_warps;
+    p.count_shape.cand = c.count_cand;
+    p.count_shape.group = c.count_group;
+    p.fill_shape.warps = c.fill_warps;
+    p.itile = c.itile;
+}
+
+// Fill grid for `mult` CTAs per SM (the cap nbl_count's planning applies).
+int fill_grid_of(const Plan &p, int64_t natoms, int mult) {
+    return std::max(1, std::min(p.num_sms * mult, (int)std::max<int64_t>((natoms + 3) / 4, 1)));
+}
+
+// The best count and fill configuration for one tile size; false on error.
+bool tune_for_tile(nbl_batch *bt, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, int itile,
+                   TuneChoice &best) {
+    const Batch &b = bt->b;
+    Plan &p = bt->p;
+    const int kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
+    TuneChoice c = best;
+    c.itile = itile;
+    apply_choice(p, c);
+    // count: shape at two waves with tickets, then the grid for the best shape
+    float best_ms = 1e30f;
+    const int warps[] = {2, 4, 8};
+    const int groups[] = {2, 4};
+    for (int w : warps) {
+        for (int cand = 0; cand <= 1; cand++) {
+            for (int g : groups) {
+                if (!b.fp32 && g != 4) continue;  // the group only shapes the FP32 sweep
+                TravShape sh;
+                sh.warps = w;
+                sh.cand = cand;
+                sh.group = g;
+                const int occ = traverse_blocks_per_sm(kModeCount, b.fp32, kind, sh);
+                if (occ <= 0) continue;
+                p.count_shape = sh;
+                p.count_mult = 2 * occ;
+                p.count_tickets = true;
+                const float ms = time_count(bt, st, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    c.count_warps = w;
+                    c.count_cand = cand;
+                    c.count_group = g;
+                    c.count_mult = 2 * occ;
+                    c.count_tickets = 1;
+                }
+            }
+        }
+    }
+    if (best_ms >= 1e30f) return false;
+    {
+        TravShape sh;
+        sh.warps = c.count_warps;
+        sh.cand = c.count_cand;
+        sh.group = c.count_group;
+        p.count_shape = sh;
+        const int occ = std::max(1, traverse_blocks_per_sm(kModeCount, b.fp32, kind, sh));
+        const int waves[] = {1, 2, 4};
+        for (int wv : waves) {
+            for (int tk = 1; tk >= 0; tk--) {
+                p.count_mult = wv * occ;
+                p.count_tickets = tk != 0;
+                const float ms = time_count(bt, st, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    c.count_mult = wv * occ;
+                    c.count_tickets = tk;
+                }
+            }
+        }
+    }
+    c.count_ms = best_ms;
+    apply_choice(p, c);
+    if (enqueue_count(p, bt->b, st) != NBL_SUCCESS) return false;
+    p.have_count = true;  // the fills below read this count's offsets
+    // fill: block size at two waves with tickets, then the grid
+    best_ms = 1e30f;
+    for (int w : warps) {
+        TravShape sh;
+        sh.warps = w;
+        const int occ = traverse_blocks_per_sm(kModeFill, b.fp32, kind, sh);
+        if (occ <= 0) continue;
+        p.fill_shape = sh;
+        p.fill_tickets = true;
+        p.fill_grid = fill_grid_of(p, b.natoms, 2 * occ);
+        const float ms = time_fill(bt, st, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            c.fill_warps = w;
+            c.fill_mult = 2 * occ;
+            c.fill_tickets = 1;
+        }
+    }
+    if (best_ms >= 1e30f) return false;
+    {
+        TravShape sh;
+        sh.warps = c.fill_warps;
+        p.fill_shape = sh;
+        const int occ = std::max(1, traverse_blocks_per_sm(kModeFill, b.fp32, kind, sh));
+        const int waves[] = {1, 2, 4};
+        for (int wv : waves) {
+            for (int tk = 1; tk >= 0; tk--) {
+                p.fill_tickets = tk != 0;
+                p.fill_grid = fill_grid_of(p, b.natoms, wv * occ);
+                const float ms = time_fill(bt, st, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    c.fill_mult = wv * occ;
+                    c.fill_tickets = tk;
+                }
+            }
+        }
+    }
+    c.fill_ms = best_ms;
+    best = c;
+    return true;
 }
 
 nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
@@ -237,7 +382,7 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         max_visit = std::max(max_visit, b.sys[s].nvisit);
     }
     char key[160];
-    std::snprintf(key, sizeof(key), "w3_sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
+    std::snprintf(key, sizeof(key), "w5_sm%d_k%d_f%d_d%d_v%d", bt->p.num_sms,
                   b.sys.empty() ? 0 : b.sys[0].cutoff_kind, b.fp32 ? 1 : 0,
                   bucket_log2(b.natoms / std::max(cells, 1.0)), bucket_log2(max_visit));
     bt->tune_key = key;
@@ -246,78 +391,33 @@ nbl_status autotune(nbl_batch *bt, cudaStream_t st) {
         tune_load_locked();
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            bt->p.count_mult = it->second.count_mult;
-            bt->p.count_group = it->second.count_group;
-            bt->p.fill_mult = it->second.fill_mult;
-            bt->p.count_tickets = it->second.count_tickets != 0;
-            bt->p.fill_tickets = it->second.fill_tickets != 0;
+            apply_choice(bt->p, it->second);
+            bt->tuned_count_ms = it->second.count_ms;
+            bt->tuned_fill_ms = it->second.fill_ms;
             return NBL_SUCCESS;
         }
     }
     cudaEvent_t e0, e1;
     NBL_CUDA(cudaEventCreate(&e0), "event");
     NBL_CUDA(cudaEventCreate(&e1), "event");
-    TuneChoice best{bt->p.count_mult, bt->p.count_group, bt->p.fill_mult,
-                    bt->p.count_tickets ? 1 : 0, bt->p.fill_tickets ? 1 : 0};
-    float best_ms = 1e30f;
-    // grids of 1, 2 and 4 full waves of each kernel's resident CTAs
-    const int waves[] = {1, 2, 4};
-    const int groups[] = {2, 4};
-    const int kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
-    for (int g : groups) {
-        if (!b.fp32 && g != 4) continue;  // the group only shapes the FP32 sweep
-        const int occ = std::max(1, traverse_blocks_per_sm(kModeCount, b.fp32, kind, g));
-        for (int wv : waves) {
-            for (int tk = 1; tk >= 0; tk--) {
-                const int m = wv * occ;
-                bt->p.count_mult = m;
-                bt->p.count_group = g;
-                bt->p.count_tickets = tk != 0;
-                const float ms = time_count(bt, st, e0, e1);
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best.count_mult = m;
-                    best.count_group = g;
-                    best.count_tickets = tk;
-                }
-            }
-        }
+    TuneChoice best;
+    bool have = false;
+    const int tiles[] = {32, 16};
+    for (int t : tiles) {
+        TuneChoice c;
+        if (!tune_for_tile(bt, st, e0, e1, t, c)) continue;
+        if (!have || c.count_ms + c.fill_ms < best.count_ms + best.fill_ms) best = c;
+        have = true;
     }
-    bt->p.count_mult = best.count_mult;
-    bt->p.count_group = best.count_group;
-    bt->p.count_tickets = best.count_tickets != 0;
-    if (enqueue_count(bt->p, bt->b, st) != NBL_SUCCESS) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return NBL_ERROR_INTERNAL;
-    }
-    bt->p.have_count = true;  // the fill below reads this count's offsets
-    best_ms = 1e30f;
-    const int focc = std::max(1, traverse_blocks_per_sm(kModeFill, b.fp32, kind));
-    for (int wv : waves) {
-        for (int tk = 1; tk >= 0; tk--) {
-            const int m = wv * focc;
-            bt->p.fill_mult = m;
-            bt->p.fill_tickets = tk != 0;
-            bt->p.fill_grid = std::max(1, std::min(bt->p.num_sms * m, (int)std::max<int64_t>(
-                                                                        (b.natoms + 3) / 4, 1)));
-            const float ms = time_fill(bt, st, e0, e1);
-            if (ms >= 1e30f) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return NBL_ERROR_INTERNAL;
-            }
-            if (ms < best_ms) {
-                best_ms = ms;
-                best.fill_mult = m;
-                best.fill_tickets = tk;
-            }
-        }
-    }
-    bt->p.fill_mult = best.fill_mult;
-    bt->p.fill_tickets = best.fill_tickets != 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (!have) {
+        apply_choice(bt->p, TuneChoice());
+        return set_error(NBL_ERROR_INTERNAL, "autotuner: no launch configuration ran");
+    }
+    apply_choice(bt->p, best);
+    bt->tuned_count_ms = best.count_ms;
+    bt->tuned_fill_ms = best.fill_ms;
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     tune_store_locked(key, best);
     return NBL_SUCCESS;
@@ -551,7 +651,7 @@ NBL_API nbl_status nbl_batch_get_config(nbl_batch *bt, int *count_mult, int *cou
                                         int *fill_mult) {
     if (!bt) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null batch");
     if (count_mult) *count_mult = bt->p.count_mult;
-    if (count_group) *count_group = bt->p.count_group;
+    if (count_group) *count_group = bt->p.count_shape.group;
     if (fill_mult) *fill_mult = bt->p.fill_mult;
     return NBL_SUCCESS;
 }
@@ -560,6 +660,15 @@ NBL_API nbl_status nbl_batch_get_tickets(nbl_batch *bt, int *count_tickets, int 
     if (!bt) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null batch");
     if (count_tickets) *count_tickets = bt->p.count_tickets ? 1 : 0;
     if (fill_tickets) *fill_tickets = bt->p.fill_tickets ? 1 : 0;
+    return NBL_SUCCESS;
+}
+
+NBL_API nbl_status nbl_batch_get_launch_config(nbl_batch *bt, nbl_launch_config *cfg,
+                                               float *count_ms, float *fill_ms) {
+    if (!bt || !cfg) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null argument");
+    launch_config_of(bt->p, cfg);
+    if (count_ms) *count_ms = bt->tuned_count_ms;
+    if (fill_ms) *fill_ms = bt->tuned_fill_ms;
     return NBL_SUCCESS;
 }
 

@@ -25,7 +25,7 @@
 // them 32 at a time against the tile's atoms (FP32 filter with an FP64 guard
 // band, or plain FP64; __ballot_sync + __popc), and the fill turns the hit
 // words into 32 pairs per round so that the FP64 epilogue and the stores run
-// with full warps and near-contiguous addresses (details below).
+// with full warps and near-contiguous addresses (details in nbl_traverse.cuh).
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -54,12 +54,6 @@ __device__ __forceinline__ int sys_of(const int64_t *__restrict__ bases, int nsy
     return lo;
 }
 
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
 // Open-addressing insert; returns the slot.  At most cap probes.
 __device__ __forceinline__ uint32_t hash_insert(unsigned long long *hkey,
                                                 unsigned long long mask,
@@ -76,21 +70,6 @@ __device__ __forceinline__ uint32_t hash_insert(unsigned long long *hkey,
     }
     atomicOr(err, kErrInternal);
     return 0;
-}
-
-__device__ __forceinline__ int2 hash_find(const unsigned long long *__restrict__ hkey,
-                                          unsigned long long mask,
-                                          const int2 *__restrict__ table,
-                                          unsigned long long key, int *err) {
-    unsigned long long h = mix64(key) & mask;
-    for (unsigned long long p = 0; p <= mask; p++) {
-        unsigned long long cur = hkey[h];
-        if (cur == key) return table[h];
-        if (cur == kHashEmpty) return make_int2(0, 0);
-        h = (h + 1) & mask;
-    }
-    atomicOr(err, kErrInternal);
-    return make_int2(0, 0);
 }
 
 }  // namespace
@@ -231,13 +210,14 @@ k_gather(GatherArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_tiles: work items = (occupied cell, 32-atom i-tile)
+// k_tiles: work items = (occupied cell, i-tile of `itile` <= 32 atoms)
 // ---------------------------------------------------------------------------
 // Splitting large cells keeps one warp from holding a whole big cell (a
 // small periodic system often is one cell) while the rest of the GPU idles.
 __global__ void __launch_bounds__(256)
 k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
-        const int2 *__restrict__ table, int2 *__restrict__ items, int *__restrict__ n_items) {
+        const int2 *__restrict__ table, int2 *__restrict__ items, int *__restrict__ n_items,
+        int itile) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int nh = *n_home;
@@ -245,7 +225,7 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
         const int h = base + threadIdx.x;
         int2 hs = make_int2(0, 0);
         if (h < nh) hs = table[home[h].tidx];
-        const int nt = (hs.y - hs.x + 31) >> 5;
+        const int nt = (hs.y - hs.x + itile - 1) / itile;
         int incl = nt;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -256,1038 +236,21 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
         int first = 0;
         if (lane == 0 && tot > 0) first = atomicAdd(n_items, tot);
         first = __shfl_sync(full, first, 0) + incl - nt;
-        for (int t = 0; t < nt; t++) items[first + t] = make_int2(h, hs.x + 32 * t);
+        for (int t = 0; t < nt; t++) items[first + t] = make_int2(h, hs.x + itile * t);
     }
 }
 
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         int2 *items, int *n_items, int64_t natoms, int num_sms,
+                         int2 *items, int *n_items, int64_t natoms, int num_sms, int itile,
                          cudaStream_t st) {
     if (natoms <= 0) return cudaSuccess;
+    if (itile < 1 || itile > 32) return cudaErrorInvalidValue;
     const int64_t blocks = std::min<int64_t>((natoms + 255) / 256, (int64_t)num_sms * 4);
-    k_tiles<<<(unsigned)blocks, 256, 0, st>>>(home, n_home, table, items, n_items);
+    k_tiles<<<(unsigned)blocks, 256, 0, st>>>(home, n_home, table, items, n_items, itile);
     count_launch();
     return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// The pair passes: k_count and k_fill
-// ---------------------------------------------------------------------------
-//
-// Both take one work item (home cell x i-tile of up to 32 atoms) per WARP
-// (each warp claims its next item with an atomic ticket, issued while the
-// current item runs; a CTA is four independent warps, so there is no
-// block-wide barrier).  Per item, one lane per visited neighbour offset
-// reads the offset vector (FP64, reference order, from the per-system visit
-// table), the wrap counts and the cell slice, and a warp scan turns slice
-// lengths into candidate positions (the "segment batch").
-//
-// k_count stages the candidates in shared memory as FP32 positions in the
-// home-cell frame (lane = segment: each copies its cell's run of sorted
-// atoms) and sweeps them against the tile's atoms, GROUP atoms per pass
-// (independent FMA chains), 32 candidates per __ballot_sync.  Each chunk's
-// hit mask is popc'ed into the atom's count and, when the item fits the mask
-// pool, stored as one 32-bit word per (atom, chunk).
-//
-// k_fill turns hit words back into pairs lane-parallel: for a window of atoms
-// it builds the prefix of the words' popcounts and keeps the atoms whose pairs
-// fit kPosTab; each word then writes its set bits' (candidate, atom) codes at
-// their output positions (lane = word, ffs), so lane L of each round finds
-// pair P = P0 + L with one shared-memory load (a single atom with more pairs
-// searches: binary search over the prefix, then an n-th-set-bit search).  The pair (exact FP64
-// D, d and S) goes to row_start + rank, so consecutive lanes write
-// consecutive slots; the next round's j-side loads are issued before this
-// round's stores.  Items without pool words (pool full, more than one segment
-// batch) recompute the words with the count's sweep first.
-namespace {
-
-constexpr int kThreads = 128;
-constexpr int kWarps = kThreads / 32;
-static_assert(kWarps == kTraverseWarps, "per-warp partial arrays are sized by kTraverseWarps");
-constexpr int kSeg = 32;         // visited offsets per batch (one per lane)
-constexpr int kITile = 32;       // atoms i per i-tile
-constexpr int kWinWords = 256;   // hit words per emission window
-constexpr int kRange = kWinWords * 32;  // candidates per emission range
-constexpr float kFarCand = 1.0e18f;     // padding candidate
-constexpr float kFarAtom = -1.0e18f;    // padding atom (never near a padding candidate)
-
-template <bool FP32>
-using CandT = typename std::conditional<FP32, float4, double4>::type;
-
-template <bool FP32>
-struct CountTile {
-    static constexpr int kCand = FP32 ? 384 : 192;
-};
-template <bool FP32>
-struct FillTile {
-    static constexpr int kCand = FP32 ? 64 : 32;
-};
-
-struct SegSmem {
-    double off[kSeg][3];
-    float off32[kSeg][3];
-    int32_t m[kSeg][3];
-    int32_t b[kSeg];
-    int32_t pref[kSeg + 1];
-};
-
-template <bool FP32>
-struct __align__(16) CountSmem {
-    SegSmem sg;
-    CandT<FP32> cand[CountTile<FP32>::kCand];
-    float4 i32[kITile];
-    int32_t iatom[kITile];
-    int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
-    int32_t icount[kITile];
-};
-
-constexpr int kCandTab = 1024;   // candidates with a segment-table entry (fill)
-constexpr int kPosTab = 640;     // pairs per window with a position table (fill)
-static_assert(kRange <= 8192 && kITile <= 32,
-              "position-table entries hold the candidate in 13 bits, the atom in 5");
-
-// Per-warp fill state, about 9.6 KB, so that five 4-warp CTAs fit an SM
-// (the force sink's sums live in a separate array of the force-sink kernel).
-template <bool FP32>
-struct __align__(16) FillSmem {
-    SegSmem sg;
-    double4 i64[kITile];
-    int4 iaux[kITile];
-    int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
-    long long icur[kITile];
-    long long abase[kITile];   // output slot of window position 0 of each window atom
-    uint32_t mw[kWinWords];
-    int32_t mpre[kWinWords + 1];
-    union {
-        uint32_t ptab[kPosTab];  // window position -> candidate | atom << 13 (small windows)
-        CandT<FP32> cand[FillTile<FP32>::kCand];  // staged candidates (recomputed words)
-    };
-    uint8_t cand_seg[kCandTab];     // segment of each of the batch's first candidates
-};
-static_assert(5 * (4 * sizeof(FillSmem<true>) + 4 * 32 * 32 + 1024) <= 233472 &&
-                  5 * (4 * sizeof(FillSmem<false>) + 4 * 32 * 32 + 1024) <= 233472,
-              "five fill CTAs per SM (force-sink sums included) fit the SM's shared memory");
-
-// Resident CTAs per SM the fill is compiled for (registers and shared memory).
-constexpr int kFillBlocks = 5;
-
-// Per-home-cell constants kept in registers.
-struct Hot {
-    float lo_rc, hi_rc, band;
-    double cutoff_sq;
-    int pbc_bits;
-    int ncut;
-    int pt_base;
-    int64_t atom_base;
-};
-
-struct Home {
-    HomeCell hc;
-    const SysDev *S;
-    int2 hs;
-    Hot H;
-    int nvisit;
-};
-
-template <bool FP32>
-__device__ __forceinline__ Home load_home(const TraverseArgs &a, int h) {
-    Home c;
-    c.hc = a.home[h];
-    c.S = a.sys + c.hc.sys;
-    const SysDev &S = *c.S;
-    c.hs = a.table[c.hc.tidx];
-    c.H.lo_rc = c.H.hi_rc = c.H.band = 0.f;
-    if (FP32) {
-        const double R = S.cutoff;
-        const double M = 2.0 * (double)a.amax[c.hc.sys] + S.off_max;
-        const double band = guard_band(M, R);
-        c.H.lo_rc = __double2float_rd(S.cutoff_sq - band);
-        c.H.hi_rc = __double2float_ru(S.cutoff_sq + band);
-        c.H.band = __double2float_ru(band);
-    }
-    c.H.cutoff_sq = S.cutoff_sq;
-    c.H.pbc_bits = (S.pbc[0] ? 1 : 0) | (S.pbc[1] ? 2 : 0) | (S.pbc[2] ? 4 : 0);
-    c.H.ncut = S.ncutoffs;
-    c.H.pt_base = S.pt_base;
-    c.H.atom_base = S.atom_base;
-    c.nvisit = S.nvisit;
-    return c;
-}
-
-__device__ __forceinline__ int2 cell_lookup(const TraverseArgs &a, const SysDev &S,
-                                            int sysid, int32_t c0, int32_t c1,
-                                            int32_t c2) {
-    const int64_t lin = (int64_t)c0 + (int64_t)S.n[0] *
-                                          ((int64_t)c1 + (int64_t)S.n[1] * c2);
-    if (a.grid != kGridHashed) return a.table[S.cell_base + lin];
-    const unsigned long long key =
-        ((unsigned long long)sysid << kHashSysShift) | (unsigned long long)lin;
-    return hash_find(a.hkey, a.hmask, a.table, key, a.err);
-}
-
-// Offset vector of cell offset d (neighbour_visit.hh:67,73,80):
-// off3 = z b3; off2 = off3 + y b2; off = off2 + x b1, in FP64 without FMA.
-__device__ __forceinline__ void visit_offset(const SysDev &S, const int d[3], double o[3]) {
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        double v = dmul((double)d[2], S.bin[2][k]);
-        v = dadd(v, dmul((double)d[1], S.bin[1][k]));
-        v = dadd(v, dmul((double)d[0], S.bin[0][k]));
-        o[k] = v;
-    }
-}
-
-// Segment batch vb of a home cell: one lane per visited offset
-// (neighbour_visit.hh:63-84).  Returns the batch size, its candidate total
-// and the index of the zero-offset segment (-1 if not in this batch).
-__device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &a,
-                                               const Home &c, int vb, int lane, int &nseg,
-                                               int &total, int &zs) {
-    const unsigned full = 0xffffffffu;
-    const SysDev &S = *c.S;
-    const int nx = S.nscan[0], ny = S.nscan[1], nz = S.nscan[2];
-    const int wx = 2 * nx + 1, wy = 2 * ny + 1;
-    nseg = min(kSeg, c.nvisit - vb);
-    int len = 0;
-    bool zero = false;
-    if (lane < nseg) {
-        const int v = vb + lane;
-        int off3[3];
-        double offd[3];
-        float off32[3];
-        if (S.visit_base >= 0) {
-            const VisitDev &e = a.visit[S.visit_base + v];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                off3[k] = e.d[k];
-                offd[k] = e.off[k];
-                off32[k] = e.off32[k];
-            }
-        } else {
-            const int xr = v % wx, rest = v / wx;
-            const int yr = rest % wy, zr = rest / wy;
-            off3[0] = xr - nx;
-            off3[1] = yr - ny;
-            off3[2] = zr - nz;
-            visit_offset(S, off3, offd);
-#pragma unroll
-            for (int k = 0; k < 3; k++) off32[k] = __double2float_rn(offd[k]);
-        }
-        int32_t cj[3], m[3];
-        bool ok = true;
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            int32_t x = c.hc.c[k] + off3[k];
-            m[k] = 0;
-            if (S.pbc[k]) {
-                const int32_t n = S.n[k];
-                if (x < 0 && x >= -n) {
-                    m[k] = -1;
-                    x += n;
-                } else if (x >= n && x < 2 * n) {
-                    m[k] = 1;
-                    x -= n;
-                } else if (x < 0 || x >= n) {
-                    m[k] = floor_div(x, n);
-                    x -= m[k] * n;
-                }
-            } else if (x < 0 || x >= S.n[k]) {
-                ok = false;
-            }
-            cj[k] = x;
-        }
-        int2 sl = make_int2(0, 0);
-        if (ok) sl = cell_lookup(a, S, c.hc.sys, cj[0], cj[1], cj[2]);
-        len = sl.y - sl.x;
-        sg.b[lane] = sl.x;
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            sg.off[lane][k] = offd[k];
-            sg.off32[lane][k] = off32[k];
-            sg.m[lane][k] = m[k];
-        }
-        zero = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
-    }
-    int incl = len;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int o = __shfl_up_sync(full, incl, d);
-        if (lane >= d) incl += o;
-    }
-    total = __shfl_sync(full, incl, 31);
-    if (lane < nseg) sg.pref[lane] = incl - len;
-    if (lane == 0) sg.pref[nseg] = total;
-    const unsigned zm = __ballot_sync(full, zero);
-    zs = zm ? __ffs(zm) - 1 : -1;
-    __syncwarp();
-}
-
-// Segment of candidate kk of the current batch.
-__device__ __forceinline__ int seg_of(const SegSmem &sg, int nseg, int kk) {
-    int lo = 0, hi = nseg - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (sg.pref[mid] <= kk)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-// Stage candidates kb .. kb+nk of the batch, padded to nkp with far points.
-// Short cell runs (the usual case): lane = segment, each copying its cell's
-// run of consecutive sorted atoms.  Long runs: lane = candidate, the lane's
-// segment found once by search and then advanced as its candidate grows.
-template <bool FP32>
-__device__ __forceinline__ void stage_segs(CandT<FP32> *cand, const SegSmem &sg,
-                                           const TraverseArgs &a, int nseg, int kb, int nk,
-                                           int nkp, int lane) {
-    __syncwarp();
-    if (sg.pref[nseg] > 48 * nseg) {
-        int seg = lane < nk ? seg_of(sg, nseg, kb + lane) : 0;
-        for (int k = lane; k < nk; k += 32) {
-            const int kk = kb + k;
-            while (seg + 1 < nseg && sg.pref[seg + 1] <= kk) seg++;
-            const int sj = sg.b[seg] + (kk - sg.pref[seg]);
-            if constexpr (FP32) {
-                const float4 p = a.pos32[sj];
-                cand[k] = make_float4(p.x + sg.off32[seg][0], p.y + sg.off32[seg][1],
-                                      p.z + sg.off32[seg][2], p.w);
-            } else {
-                cand[k] = a.pos64[sj];
-            }
-        }
-    } else if (lane < nseg) {
-        const int s0 = max(sg.pref[lane], kb), s1 = min(sg.pref[lane + 1], kb + nk);
-        const int jb = sg.b[lane] - sg.pref[lane];
-        if constexpr (FP32) {
-            const float ox = sg.off32[lane][0], oy = sg.off32[lane][1], oz = sg.off32[lane][2];
-#pragma unroll 4
-            for (int kk = s0; kk < s1; kk++) {
-                const float4 p = a.pos32[jb + kk];
-                cand[kk - kb] = make_float4(p.x + ox, p.y + oy, p.z + oz, p.w);
-            }
-        } else {
-#pragma unroll 4
-            for (int kk = s0; kk < s1; kk++) cand[kk - kb] = a.pos64[jb + kk];
-        }
-    }
-    for (int k = nk + lane; k < nkp; k += 32) {
-        if constexpr (FP32)
-            cand[k] = make_float4(kFarCand, kFarCand, kFarCand, 0.f);
-        else
-            cand[k] = make_double4(kFarCand, kFarCand, kFarCand, 0.0);
-    }
-    __syncwarp();
-}
-
-// The reference's exact FP64 inclusion test (neighbour_visit.hh:88-109).
-template <int KIND>
-__device__ __forceinline__ bool exact_inside(const Hot &H, const TraverseArgs &a,
-                                             const double4 &pi, const double4 &pj,
-                                             const double *off, float ti_bits,
-                                             float tj_bits) {
-    const double dx = dadd(dsub(pj.x, pi.x), off[0]);
-    const double dy = dadd(dsub(pj.y, pi.y), off[1]);
-    const double dz = dadd(dsub(pj.z, pi.z), off[2]);
-    const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-    if (!(r2 < H.cutoff_sq)) return false;
-    if (KIND == kCutPerAtom) {
-        const double cc = dadd(pi.w, pj.w);
-        return r2 < dmul(cc, cc);
-    }
-    if (KIND == kCutPerType) {
-        const int ti = __float_as_int(ti_bits), tj = __float_as_int(tj_bits);
-        if (ti >= 0 && ti < H.ncut && tj >= 0 && tj < H.ncut)
-            return r2 < a.pt64[H.pt_base + ti * H.ncut + tj];
-    }
-    return true;
-}
-
-// Guard-band candidate kk of the batch for atom si, decided in FP64 (cold).
-template <int KIND>
-__device__ __noinline__ bool resolve_exact(const SegSmem &sg, const TraverseArgs &a,
-                                           const Hot &H, int nseg, int kk, int si,
-                                           float wi) {
-    const int seg = seg_of(sg, nseg, kk);
-    const int32_t sj = sg.b[seg] + (kk - sg.pref[seg]);
-    return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], sg.off[seg], wi,
-                              a.pos32[sj].w);
-}
-
-// FP32 thresholds for one (atom, candidate) pair.
-template <int KIND>
-__device__ __forceinline__ void thresholds(const Hot &H, const TraverseArgs &a, float wi,
-                                           float wj, float &lo, float &hi) {
-    lo = H.lo_rc;
-    hi = H.hi_rc;
-    if (KIND == kCutPerAtom) {
-        const float cc = wi + wj;
-        const float t = cc * cc;
-        lo = fminf(lo, t - H.band);
-        hi = fminf(hi, t + H.band);
-    } else if (KIND == kCutPerType) {
-        const int ti = __float_as_int(wi), tj = __float_as_int(wj);
-        if (ti >= 0 && ti < H.ncut && tj >= 0 && tj < H.ncut) {
-            const float t = a.pt32[H.pt_base + ti * H.ncut + tj];
-            lo = fminf(lo, t - H.band);
-            hi = fminf(hi, t + H.band);
-        }
-    }
-}
-
-// Hit mask of one staged 32-candidate chunk (tile positions k0..k0+31) for one
-// atom: FP32 filter + FP64 guard band, or plain FP64.
-template <bool FP32, int KIND>
-__device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const SegSmem &sg,
-                                               const TraverseArgs &a, const Hot &H,
-                                               int nseg, int kb, int k0, int lane,
-                                               int kself_tile, int si, const float4 &pi32,
-                                               const double4 &pi64) {
-    const unsigned full = 0xffffffffu;
-    const int k = k0 + lane;
-    const bool notself = k != kself_tile;
-    if constexpr (FP32) {
-        const float4 cv = cand[k];
-        const float dx = cv.x - pi32.x;
-        const float dy = cv.y - pi32.y;
-        const float dz = cv.z - pi32.z;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        float lo, hi;
-        thresholds<KIND>(H, a, pi32.w, cv.w, lo, hi);
-        unsigned mask = __ballot_sync(full, (r2 < lo) && notself);
-        const bool amb = !(r2 < lo) && (r2 < hi) && notself;
-        if (__any_sync(full, amb)) {
-            bool h2 = false;
-            if (amb) h2 = resolve_exact<KIND>(sg, a, H, nseg, kb + k, si, pi32.w);
-            mask |= __ballot_sync(full, h2);
-        }
-        return mask;
-    } else {
-        bool hit = false;
-        const double4 pj = cand[k];
-        if (notself && pj.x != (double)kFarCand) {
-            const int seg = seg_of(sg, nseg, kb + k);
-            float tj = 0.f;
-            if (KIND == kCutPerType) tj = a.pos32[sg.b[seg] + (kb + k - sg.pref[seg])].w;
-            hit = exact_inside<KIND>(H, a, pi64, pj, sg.off[seg], pi32.w, tj);
-        }
-        return __ballot_sync(full, hit);
-    }
-}
-
-// The warp's first work item: a ticket from a.item_next, else the warp index.
-__device__ __forceinline__ int first_item(const TraverseArgs &a, int gwarp, int lane) {
-    if (a.item_next == nullptr) return gwarp;
-    int t = 0;
-    if (lane == 0) t = atomicAdd(a.item_next, 1);
-    return __shfl_sync(0xffffffffu, t, 0);
-}
-
-// The warp's next work item: lane 0's ticket `pend` (claimed at the start of
-// the current item), else a fixed stride.
-__device__ __forceinline__ int next_item(const TraverseArgs &a, int it, int nwarps, int pend) {
-    if (a.item_next == nullptr) return it + nwarps;
-    return __shfl_sync(0xffffffffu, pend, 0);
-}
-
-// Position of the (r+1)-th set bit of w (r < popc(w)).
-__device__ __forceinline__ int nth_set_bit(unsigned w, int r) {
-    int pos = 0;
-#pragma unroll
-    for (int sh = 16; sh > 0; sh >>= 1) {
-        const unsigned low = w & ((1u << sh) - 1u);
-        const int c = __popc(low);
-        if (r >= c) {
-            r -= c;
-            w >>= sh;
-            pos += sh;
-        } else {
-            w = low;
-        }
-    }
-    return pos;
-}
-
-// w / n for 0 <= w < 2^20 and small n, without an integer division.
-__device__ __forceinline__ int div_small(int w, int n, float inv_n) {
-    int q = __float2int_rz((float)w * inv_n);
-    if (q * n > w) q--;
-    if ((q + 1) * n <= w) q++;
-    return q;
-}
-
-}  // namespace
-
-template <bool FP32, int KIND, int GROUP>
-__global__ void __launch_bounds__(kThreads, 6)
-k_count(TraverseArgs a) {
-    constexpr int kCand = CountTile<FP32>::kCand;
-    __shared__ CountSmem<FP32> smem[kWarps];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    CountSmem<FP32> &sm = smem[warp];
-    const unsigned full = 0xffffffffu;
-    const int nitems = *a.n_items;
-    const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
-
-    int pend = 0;  // lane 0: the ticket claimed while the current item runs
-    for (int it = first_item(a, gwarp, lane); it < nitems;
-         it = next_item(a, it, nwarps, pend)) {
-        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
-        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
-        const Home c = load_home<FP32>(a, item.x);
-        const Hot &H = c.H;
-        const int2 hs = c.hs;
-        long long mbase = -1;
-
-        {
-            const int ib = item.y;
-            // The tile's atoms whose original index lies in [i_lo, i_hi),
-            // compacted in order (all of them unless the rows are split).
-            int ni;
-            {
-                const int nt = min(kITile, hs.y - ib);
-                int ax = 0;
-                bool in = false;
-                if (lane < nt) {
-                    ax = a.aux[ib + lane].x;
-                    in = ax >= a.i_lo && ax < a.i_hi;
-                }
-                const unsigned im = __ballot_sync(full, in);
-                ni = __popc(im);
-                if (in) {
-                    const int c2 = __popc(im & lanemask_lt());
-                    sm.i32[c2] = a.pos32[ib + lane];
-                    sm.iatom[c2] = ax;
-                    sm.isi[c2] = ib + lane;
-                    sm.icount[c2] = 0;
-                }
-                __syncwarp();
-            }
-            if (ni == 0) continue;
-            for (int vb = 0; vb < c.nvisit; vb += kSeg) {
-                int nseg, total, zs;
-                setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
-                const int nchunks_all = (total + 31) >> 5;
-                // One word region per (work item, segment batch): (atoms of the
-                // i-tile) x (chunks of the batch's candidate list).
-                mbase = -1;
-                if (a.mask_pool != nullptr && vb / kSeg < kMaskBatches) {
-                    long long base = -1;
-                    if (lane == 0) {
-                        const long long words = (long long)ni * nchunks_all;
-                        const unsigned long long b =
-                            atomicAdd(a.mask_cursor, (unsigned long long)words);
-                        if ((long long)b + words <= a.mask_cap) base = (long long)b;
-                    }
-                    base = __shfl_sync(full, base, 0);
-                    if (lane == 0) a.home_mask[(long long)it * kMaskBatches + vb / kSeg] = base;
-                    mbase = base;
-                }
-                // candidate index of atom si itself at offset 0 is kself0 + si
-                const int kself0 = (zs >= 0) ? sm.sg.pref[zs] - sm.sg.b[zs] : INT_MIN / 2;
-
-                for (int kb = 0; kb < total; kb += kCand) {
-                    const int nk = min(kCand, total - kb);
-                    const int nkp = (nk + 31) & ~31;
-                    const int nck = nkp >> 5;
-                    stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
-                    if constexpr (FP32) {
-                        // GROUP atoms per pass over the tile
-                        for (int g0 = 0; g0 < ni; g0 += GROUP) {
-                            float4 pg[GROUP];
-                            int ks[GROUP], cnt[GROUP];
-                            unsigned mw[GROUP];
-#pragma unroll
-                            for (int g = 0; g < GROUP; g++) {
-                                const bool v = g0 + g < ni;
-                                pg[g] = v ? sm.i32[g0 + g]
-                                          : make_float4(kFarAtom, kFarAtom, kFarAtom, 0.f);
-                                ks[g] = v ? kself0 + sm.isi[g0 + g] - kb : -1;
-                                cnt[g] = 0;
-                                mw[g] = 0u;
-                            }
-                            // atoms in pairs for the packed (f32x2) arithmetic:
-                            // x - p == x + (-p) exactly, and the packed ops round
-                            // each half like the scalar fmaf chain
-                            constexpr int kHalf = GROUP / 2;
-                            float2 nx[kHalf], ny[kHalf], nz[kHalf];
-#pragma unroll
-                            for (int h = 0; h < kHalf; h++) {
-                                nx[h] = make_float2(-pg[2 * h].x, -pg[2 * h + 1].x);
-                                ny[h] = make_float2(-pg[2 * h].y, -pg[2 * h + 1].y);
-                                nz[h] = make_float2(-pg[2 * h].z, -pg[2 * h + 1].z);
-                            }
-                            // blocks of up to 32 chunks: lane L keeps chunk cb + L's hit
-                            // word of each atom; the block's counts and its pool words
-                            // are taken once at its end
-                            for (int cb = 0; cb < nck; cb += 32) {
-                                const int ce = min(nck, cb + 32);
-#pragma unroll
-                                for (int g = 0; g < GROUP; g++) mw[g] = 0u;
-                                for (int ch = cb; ch < ce; ch++) {
-                                    const int k = ch * 32 + lane;
-                                    const float4 cv = sm.cand[k];
-                                    unsigned m[GROUP];
-                                    bool amb_any = false, amb[GROUP];
-                                    float r2g[GROUP];
-                                    const float2 cx = make_float2(cv.x, cv.x);
-                                    const float2 cy = make_float2(cv.y, cv.y);
-                                    const float2 cz = make_float2(cv.z, cv.z);
-#pragma unroll
-                                    for (int h = 0; h < kHalf; h++) {
-                                        const float2 dx = __fadd2_rn(cx, nx[h]);
-                                        const float2 dy = __fadd2_rn(cy, ny[h]);
-                                        const float2 dz = __fadd2_rn(cz, nz[h]);
-                                        const float2 r2 = __ffma2_rn(
-                                            dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                        r2g[2 * h] = r2.x;
-                                        r2g[2 * h + 1] = r2.y;
-                                    }
-#pragma unroll
-                                    for (int g = 0; g < GROUP; g++) {
-                                        const float r2 = r2g[g];
-                                        float lo, hi;
-                                        thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
-                                        const bool notself = k != ks[g];
-                                        m[g] = __ballot_sync(full, (r2 < lo) && notself);
-                                        amb[g] = !(r2 < lo) && (r2 < hi) && notself;
-                                        amb_any |= amb[g];
-                                    }
-                                    if (__any_sync(full, amb_any)) {
-#pragma unroll
-                                        for (int g = 0; g < GROUP; g++) {
-                                            bool h2 = false;
-                                            if (amb[g])
-                                                h2 = resolve_exact<KIND>(sm.sg, a, H, nseg,
-                                                                         kb + k, sm.isi[g0 + g],
-                                                                         pg[g].w);
-                                            m[g] |= __ballot_sync(full, h2);
-                                        }
-                                    }
-                                    const bool mine = lane == ch - cb;
-#pragma unroll
-                                    for (int g = 0; g < GROUP; g++) mw[g] = mine ? m[g] : mw[g];
-                                }
-#pragma unroll
-                                for (int g = 0; g < GROUP; g++)
-                                    cnt[g] += (int)__reduce_add_sync(full, (unsigned)__popc(mw[g]));
-                                if (mbase >= 0 && lane < ce - cb) {
-                                    const long long w0 = mbase + (kb >> 5) + cb + lane;
-#pragma unroll
-                                    for (int g = 0; g < GROUP; g++) {
-                                        if (g0 + g < ni)
-                                            a.mask_pool[w0 + (long long)(g0 + g) * nchunks_all] =
-                                                mw[g];
-                                    }
-                                }
-                            }
-                            if (lane < GROUP && g0 + lane < ni) {
-                                int cg = cnt[0];
-#pragma unroll
-                                for (int g = 1; g < GROUP; g++)
-                                    if (lane == g) cg = cnt[g];
-                                sm.icount[g0 + lane] += cg;
-                            }
-                            __syncwarp();
-                        }
-                    } else {
-                        for (int il = 0; il < ni; il++) {
-                            const int si = sm.isi[il];
-                            const float4 pi32 = sm.i32[il];
-                            const double4 pi64 = a.pos64[si];
-                            const int kself_tile = kself0 + si - kb;
-                            int cnt = 0;
-                            unsigned mword = 0;
-                            for (int ch = 0; ch < nck; ch++) {
-                                const unsigned mask = chunk_mask<FP32, KIND>(
-                                    sm.cand, sm.sg, a, H, nseg, kb, ch * 32, lane, kself_tile,
-                                    si, pi32, pi64);
-                                cnt += __popc(mask);
-                                mword = (lane == (ch & 31)) ? mask : mword;
-                                if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
-                                    if (lane <= (ch & 31))
-                                        a.mask_pool[mbase + (long long)il * nchunks_all +
-                                                    (kb >> 5) + (ch & ~31) + lane] = mword;
-                                }
-                            }
-                            if (lane == 0) sm.icount[il] += cnt;
-                            __syncwarp();
-                        }
-                    }
-                }
-            }
-            if (lane < ni) a.counts[sm.iatom[lane]] = sm.icount[lane];
-            __syncwarp();
-        }
-    }
-}
-
-// Segment of candidate kk of the batch: from the table, else by search.
-template <bool FP32>
-__device__ __forceinline__ int seg_of_tab(const FillSmem<FP32> &sm, int nseg, int kk) {
-    return kk < kCandTab ? (int)sm.cand_seg[kk] : seg_of(sm.sg, nseg, kk);
-}
-
-// One output pair in flight: where it goes and the j-side data it needs.
-struct PairWork {
-    bool act;
-    int il, seg;
-    long long slot;
-    double4 pj;
-    int4 aj;
-};
-
-// Map window position P to its pair and issue the j-side loads.
-template <bool FP32>
-__device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
-                                               const TraverseArgs &a, int nseg, int nchunks,
-                                               int nw, int nch, float inv_nch, int kr,
-                                               int a0, int total_w, int P, bool tab) {
-    PairWork w;
-    w.act = P < total_w;
-    w.il = 0;
-    w.seg = 0;
-    w.slot = 0;
-    if (w.act) {
-        int al, kk;
-        if (tab) {
-            const uint32_t e = sm.ptab[P];
-            al = (int)(e >> 13);
-            kk = kr + (int)(e & 8191u);
-        } else {
-            int lo = 0, hi = nw - 1;  // last word with mpre <= P
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sm.mpre[mid] <= P)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            const int bit = nth_set_bit(sm.mw[lo], P - sm.mpre[lo]);
-            al = div_small(lo, nch, inv_nch);
-            kk = kr + (lo - al * nch) * 32 + bit;
-        }
-        w.il = a0 + al;
-        w.slot = sm.abase[al] + P;
-        w.seg = seg_of_tab(sm, nseg, kk);
-        const int32_t sj = sm.sg.b[w.seg] + (kk - sm.sg.pref[w.seg]);
-        w.pj = a.pos64[sj];
-        w.aj = a.aux[sj];
-    }
-    return w;
-}
-
-// Compute and store one pair (exact FP64 D and d, S, i, j).  ALL5: all five
-// outputs requested and no neighbour matrix (no per-pair output checks).
-template <bool FP32, bool ALL5>
-__device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const TraverseArgs &a,
-                                           const Hot &H, const PairWork &w) {
-    if (!w.act) return;
-    const double4 pi = sm.i64[w.il];
-    const int4 ai = sm.iaux[w.il];
-    const int seg = w.seg;
-    const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
-    const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
-    const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
-    const int32_t jl = (int32_t)(w.aj.x - H.atom_base);
-    if (!ALL5 && a.mat_k > 0) {
-        const long long rank = w.slot - (long long)a.offsets[ai.x];
-        if (rank < a.mat_k) {
-            const long long m = (long long)ai.x * a.mat_k + rank;
-            a.mat_idx[m] = jl;
-            a.mat_dist[3 * m + 0] = dx;
-            a.mat_dist[3 * m + 1] = dy;
-            a.mat_dist[3 * m + 2] = dz;
-        }
-        return;
-    }
-    const long long slot = w.slot;
-    if (slot >= a.capacity) {
-        atomicOr(a.err, kErrCapacity);
-        return;
-    }
-    if (ALL5 || a.first) __stcs(a.first + slot, (int32_t)(ai.x - H.atom_base));
-    if (ALL5 || a.second) __stcs(a.second + slot, jl);
-    if (ALL5 || a.absdist) {
-        const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-        __stcs(a.absdist + slot, __dsqrt_rn(r2));
-    }
-    if (ALL5 || a.distvec) {
-        double *D = a.distvec + 3 * slot;
-        __stcs(D, dx);
-        __stcs(D + 1, dy);
-        __stcs(D + 2, dz);
-    }
-    if (ALL5 || a.shift) {
-        int32_t *Sv = a.shift + 3 * slot;
-        __stcs(Sv, ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0]);
-        __stcs(Sv + 1, ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1]);
-        __stcs(Sv + 2, ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + sm.sg.m[seg][2]);
-    }
-}
-
-// Force sink: one round of pairs, all 32 lanes.  Each active lane forms its
-// pair's Lennard-Jones force on atom i from the exact FP64 D (the reference's
-// operation order, as the stored D), U = 4 eps ((sigma/r)^12 - (sigma/r)^6)
-// cut at the list's cutoff, F_i = -24 eps s6 (2 s6 - 1) D / r^2 with
-// s6 = (sigma^2 / r^2)^3 (lj_langevin_gpu.cu:59-74 with eps = sigma = 1); the
-// lanes' forces and energy shares (1/2 U per directed pair) are summed per
-// atom (runs of equal i are contiguous) and the run's last lane adds them to
-// the tile's shared-memory sums.
-template <bool FP32>
-__device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc)[4],
-                                         const TraverseArgs &a, const PairWork &w, int lane) {
-    const unsigned full = 0xffffffffu;
-    double f0 = 0.0, f1 = 0.0, f2 = 0.0, e = 0.0;
-    const int il = w.act ? w.il : -1;
-    if (w.act) {
-        const double4 pi = sm.i64[w.il];
-        const int seg = w.seg;
-        const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
-        const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
-        const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
-        const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-        const double ir2 = 1.0 / r2;
-        const double s2 = a.lj_sig2 * ir2;
-        const double s6 = s2 * s2 * s2;
-        const double coef = -a.lj_eps24 * ir2 * s6 * (2.0 * s6 - 1.0);
-        f0 = coef * dx;
-        f1 = coef * dy;
-        f2 = coef * dz;
-        e = 0.5 * a.lj_eps4 * (s6 * s6 - s6);
-    }
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const double t0 = __shfl_up_sync(full, f0, d);
-        const double t1 = __shfl_up_sync(full, f1, d);
-        const double t2 = __shfl_up_sync(full, f2, d);
-        const double t3 = __shfl_up_sync(full, e, d);
-        const int ii = __shfl_up_sync(full, il, d);
-        if (lane >= d && ii == il) {
-            f0 += t0;
-            f1 += t1;
-            f2 += t2;
-            e += t3;
-        }
-    }
-    const int inext = __shfl_down_sync(full, il, 1);
-    if (il >= 0 && (lane == 31 || inext != il)) {
-        facc[il][0] += f0;
-        facc[il][1] += f1;
-        facc[il][2] += f2;
-        facc[il][3] += e;
-    }
-    __syncwarp();
-}
-
-template <bool FP32, int KIND, bool LJ, bool ALL5>
-__global__ void __launch_bounds__(kThreads, kFillBlocks)
-k_fill(TraverseArgs a) {
-    constexpr int kCand = FillTile<FP32>::kCand;
-    __shared__ FillSmem<FP32> smem[kWarps];
-    // force sink: each warp's tile force and energy sums
-    __shared__ double facc_all[LJ ? kWarps * kITile : 1][4];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    FillSmem<FP32> &sm = smem[warp];
-    double(*facc)[4] = facc_all + (LJ ? warp * kITile : 0);
-    const unsigned full = 0xffffffffu;
-    const int nitems = *a.n_items;
-    const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
-
-    int pend = 0;  // lane 0: the ticket claimed while the current item runs
-    for (int it = first_item(a, gwarp, lane); it < nitems;
-         it = next_item(a, it, nwarps, pend)) {
-        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
-        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
-        const Home c = load_home<FP32>(a, item.x);
-        const Hot &H = c.H;
-        const int2 hs = c.hs;
-
-        {
-            const int ib = item.y;
-            int ni;
-            {
-                const int nt = min(kITile, hs.y - ib);
-                int4 ax = make_int4(0, 0, 0, 0);
-                bool in = false;
-                if (lane < nt) {
-                    ax = a.aux[ib + lane];
-                    in = ax.x >= a.i_lo && ax.x < a.i_hi;
-                }
-                const unsigned im = __ballot_sync(full, in);
-                ni = __popc(im);
-                if (in) {
-                    const int c2 = __popc(im & lanemask_lt());
-                    const int si = ib + lane;
-                    sm.i64[c2] = a.pos64[si];
-                    sm.iaux[c2] = ax;
-                    sm.isi[c2] = si;
-                    sm.icur[c2] = (long long)a.offsets[ax.x];
-                    if (LJ) facc[c2][0] = facc[c2][1] = facc[c2][2] = facc[c2][3] = 0.0;
-                }
-                __syncwarp();
-            }
-            if (ni == 0) continue;
-            for (int vb = 0; vb < c.nvisit; vb += kSeg) {
-                int nseg, total, zs;
-                setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
-                const int nchunks = (total + 31) >> 5;
-                const long long mbase =
-                    (a.mask_pool != nullptr && vb / kSeg < kMaskBatches)
-                        ? a.home_mask[(long long)it * kMaskBatches + vb / kSeg]
-                        : -1ll;
-                // segment of each tabled candidate: lane = segment
-                if (lane < nseg) {
-                    const int e = min(sm.sg.pref[lane + 1], kCandTab);
-                    for (int k = sm.sg.pref[lane]; k < e; k++) sm.cand_seg[k] = (uint8_t)lane;
-                }
-                __syncwarp();
-                const int kself0 = (zs >= 0) ? sm.sg.pref[zs] - sm.sg.b[zs] : INT_MIN / 2;
-
-                for (int kr = 0; kr < total; kr += kRange) {
-                    const int nrange = min(kRange, total - kr);
-                    const int nch = (nrange + 31) >> 5;
-                    const float inv_nch = 1.0f / (float)nch;
-                    const int win = max(1, kWinWords / nch);
-                    for (int a0 = 0; a0 < ni;) {
-                        int na = min(win, ni - a0);
-                        int nw = na * nch;
-                        // --- the window's hit words ---------------------------------
-                        if (mbase >= 0) {
-                            for (int w = lane; w < nw; w += 32) {
-                                const int al = div_small(w, nch, inv_nch);
-                                sm.mw[w] = a.mask_pool[mbase + (long long)(a0 + al) * nchunks +
-                                                       (kr >> 5) + (w - al * nch)];
-                            }
-                        } else {
-                            for (int kt = 0; kt < nrange; kt += kCand) {
-                                const int nk = min(kCand, nrange - kt);
-                                const int nkp = (nk + 31) & ~31;
-                                stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
-                                for (int al = 0; al < na; al++) {
-                                    const int il = a0 + al, si = sm.isi[il];
-                                    const float4 pi32 = a.pos32[si];
-                                    const double4 pi64 = sm.i64[il];
-                                    const int kself_tile = kself0 + si - (kr + kt);
-                                    for (int ch = 0; ch < (nkp >> 5); ch++) {
-                                        const unsigned mask = chunk_mask<FP32, KIND>(
-                                            sm.cand, sm.sg, a, H, nseg, kr + kt, ch * 32, lane,
-                                            kself_tile, si, pi32, pi64);
-                                        if (lane == 0) sm.mw[al * nch + (kt >> 5) + ch] = mask;
-                                    }
-                                }
-                            }
-                        }
-                        __syncwarp();
-                        // --- prefix of the words' popcounts ---------------------------
-                        int carry = 0;
-                        for (int w0 = 0; w0 < nw; w0 += 32) {
-                            const int w = w0 + lane;
-                            const int p = (w < nw) ? __popc(sm.mw[w]) : 0;
-                            int incl = p;
-#pragma unroll
-                            for (int d = 1; d < 32; d <<= 1) {
-                                const int o = __shfl_up_sync(full, incl, d);
-                                if (lane >= d) incl += o;
-                            }
-                            if (w < nw) sm.mpre[w] = carry + incl - p;
-                            carry += __shfl_sync(full, incl, 31);
-                        }
-                        if (lane == 0) sm.mpre[nw] = carry;
-                        __syncwarp();
-                        // --- a window over the position table keeps only the atoms
-                        //     whose pairs fit it (at least one); the next window
-                        //     starts at the first atom left out ---------------------
-                        if (carry > kPosTab && na > 1) {
-                            const bool fits = lane >= 1 && lane <= na &&
-                                              sm.mpre[lane * nch] <= kPosTab;
-                            na = max(1, __popc(__ballot_sync(full, fits)));
-                            nw = na * nch;
-                            carry = sm.mpre[nw];
-                        }
-                        // per-atom output base: slot = abase[atom] + window position
-                        if (lane < na) sm.abase[lane] = sm.icur[a0 + lane] - sm.mpre[lane * nch];
-                        __syncwarp();
-                        // --- small windows: each word writes its bits' positions into
-                        //     a table (lane = word, ffs over its set bits), so a lane
-                        //     finds its pair with one shared-memory load --------------
-                        const bool tab = carry <= kPosTab;
-                        if (tab) {
-                            for (int w = lane; w < nw; w += 32) {
-                                unsigned word = sm.mw[w];
-                                int pos = sm.mpre[w];
-                                const int al = div_small(w, nch, inv_nch);
-                                const uint32_t base =
-                                    (uint32_t)((w - al * nch) * 32) | ((uint32_t)al << 13);
-                                while (word) {
-                                    const int b = __ffs(word) - 1;
-                                    word &= word - 1u;
-                                    sm.ptab[pos++] = base | (uint32_t)b;
-                                }
-                            }
-                            __syncwarp();
-                        }
-                        // --- emission, software-pipelined: the next round's j-side
-                        //     loads are in flight while the current round computes ----
-                        PairWork cur = fetch_pair<FP32>(sm, a, nseg, nchunks, nw, nch,
-                                                        inv_nch, kr, a0, carry, lane, tab);
-                        for (int P0 = 0; P0 < carry; P0 += 32) {
-                            const PairWork nxt = fetch_pair<FP32>(sm, a, nseg, nchunks, nw,
-                                                                  nch, inv_nch, kr, a0, carry,
-                                                                  P0 + 32 + lane, tab);
-                            if (LJ)
-                                lj_round<FP32>(sm, facc, a, cur, lane);
-                            else
-                                store_pair<FP32, ALL5>(sm, a, H, cur);
-                            cur = nxt;
-                        }
-                        __syncwarp();
-                        if (lane < na)
-                            sm.icur[a0 + lane] += sm.mpre[(lane + 1) * nch] - sm.mpre[lane * nch];
-                        __syncwarp();
-                        a0 += na;
-                    }
-                }
-            }
-            // --- fill must land exactly on the next row; matrix row lengths --------
-            if (lane < ni) {
-                const int ax = sm.iaux[lane].x;
-                const long long end = (long long)a.offsets[ax + 1];
-                if (sm.icur[lane] != end) atomicOr(a.err, kErrInternal);
-                if (a.mat_k > 0) {
-                    const long long deg = end - (long long)a.offsets[ax];
-                    a.mat_count[ax] = (int32_t)deg;
-                    if (deg > a.mat_k) atomicOr(a.mat_overflow, 1);
-                }
-                if (LJ) {
-                    a.lj_force[3 * (long long)ax + 0] = facc[lane][0];
-                    a.lj_force[3 * (long long)ax + 1] = facc[lane][1];
-                    a.lj_force[3 * (long long)ax + 2] = facc[lane][2];
-                    a.lj_energy[ax] = facc[lane][3];
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
-
-#define NBL_INST(F, K)                                            \
-    template __global__ void k_count<F, K, 2>(TraverseArgs);      \
-    template __global__ void k_count<F, K, 4>(TraverseArgs);      \
-    template __global__ void k_fill<F, K, false, false>(TraverseArgs); \
-    template __global__ void k_fill<F, K, true, false>(TraverseArgs);
-NBL_INST(true, kCutScalar)
-NBL_INST(true, kCutPerAtom)
-NBL_INST(true, kCutPerType)
-NBL_INST(false, kCutScalar)
-NBL_INST(false, kCutPerAtom)
-NBL_INST(false, kCutPerType)
-#undef NBL_INST
-template __global__ void k_fill<true, kCutScalar, false, true>(TraverseArgs);
-template __global__ void k_fill<true, kCutPerAtom, false, true>(TraverseArgs);
-template __global__ void k_fill<true, kCutPerType, false, true>(TraverseArgs);
 
 // One block per system with a visit table: its visited offsets in the
 // traversal's z/y/x order (neighbour_visit.hh:63-84).
@@ -1371,116 +334,53 @@ cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-namespace {
+// ---------------------------------------------------------------------------
+// pair-pass dispatch (kernels: nbl_traverse.cuh, instantiated in nbl_trav_*.cu)
+// ---------------------------------------------------------------------------
 
-template <typename K>
-int occupancy_of(K kern) {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThreads, 0) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return n;
+bool traverse_shape_ok(int mode, bool fp32, const TravShape &s) {
+    if (s.warps != 2 && s.warps != 4 && s.warps != 8) return false;
+    if (mode != kModeCount) return true;
+    return (s.cand == 0 || s.cand == 1) && (!fp32 || s.group == 2 || s.group == 4);
 }
 
-template <bool F, int K>
-int occupancy_fk(int mode, int group, bool lj) {
-    if (mode == kModeCount) return group == 2 ? occupancy_of(k_count<F, K, 2>)
-                                              : occupancy_of(k_count<F, K, 4>);
-    return lj ? occupancy_of(k_fill<F, K, true, false>)
-              : occupancy_of(k_fill<F, K, false, false>);
-}
-
-}  // namespace
-
-int traverse_blocks_per_sm(int mode, bool fp32, int kind, int group, bool lj) {
-    // cached per device and kernel
+int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape, bool lj) {
+    // cached per device, pass, precision, kind and shape
     constexpr int kDev = 16;
-    static std::atomic<int> cache[kDev][2][2][3][2][2];
+    static std::atomic<int> cache[kDev][2][2][3][3][2][2][2];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDev) {
         cudaGetLastError();
         dev = -1;
     }
-    const int mi = mode == kModeCount ? 0 : 1, fi = fp32 ? 1 : 0, gi = group == 2 ? 0 : 1;
+    const int mi = mode == kModeCount ? 0 : 1, fi = fp32 ? 1 : 0;
     const int ki = kind == kCutPerAtom ? 1 : (kind == kCutPerType ? 2 : 0), li = lj ? 1 : 0;
+    const int wi = shape.warps == 2 ? 0 : (shape.warps == 8 ? 2 : 1);
+    const int ci = shape.cand != 0 ? 1 : 0;
+    const int gi = shape.group == 2 ? 0 : 1;
     if (dev >= 0) {
-        const int c = cache[dev][mi][fi][ki][gi][li].load(std::memory_order_relaxed);
+        const int c = cache[dev][mi][fi][ki][wi][ci][gi][li].load(std::memory_order_relaxed);
         if (c > 0) return c;
     }
     int n = 0;
-    if (fp32) {
-        n = ki == 1 ? occupancy_fk<true, kCutPerAtom>(mode, group, lj)
-                    : (ki == 2 ? occupancy_fk<true, kCutPerType>(mode, group, lj)
-                               : occupancy_fk<true, kCutScalar>(mode, group, lj));
-    } else {
-        n = ki == 1 ? occupancy_fk<false, kCutPerAtom>(mode, group, lj)
-                    : (ki == 2 ? occupancy_fk<false, kCutPerType>(mode, group, lj)
-                               : occupancy_fk<false, kCutScalar>(mode, group, lj));
-    }
-    if (dev >= 0 && n > 0) cache[dev][mi][fi][ki][gi][li].store(n, std::memory_order_relaxed);
+    if (mode == kModeCount)
+        n = fp32 ? occupancy_count_fp32(kind, shape) : occupancy_count_fp64(kind, shape);
+    else
+        n = fp32 ? occupancy_fill_fp32(kind, shape, lj) : occupancy_fill_fp64(kind, shape, lj);
+    if (dev >= 0 && n > 0)
+        cache[dev][mi][fi][ki][wi][ci][gi][li].store(n, std::memory_order_relaxed);
     return n;
 }
 
-namespace {
-
-template <bool F, int K>
-void launch_fill(const TraverseArgs &a, int grid, cudaStream_t st) {
-    if (a.lj_force != nullptr) {
-        k_fill<F, K, true, false><<<grid, kThreads, 0, st>>>(a);
-        return;
-    }
-    if constexpr (F) {
-        if (a.first && a.second && a.distvec && a.absdist && a.shift && a.mat_k == 0) {
-            k_fill<F, K, false, true><<<grid, kThreads, 0, st>>>(a);
-            return;
-        }
-    }
-    k_fill<F, K, false, false><<<grid, kThreads, 0, st>>>(a);
-}
-
-}  // namespace
-
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
-                            int grid, cudaStream_t st, int group) {
+                            int grid, cudaStream_t st, const TravShape &shape) {
     if (grid <= 0) return cudaSuccess;
-    if (a.item_next != nullptr) {
-        const cudaError_t e = cudaMemsetAsync(a.item_next, 0, sizeof(int), st);
-        if (e != cudaSuccess) return e;
-    }
-#define NBL_GO_C(F, K)                                                     \
-    do {                                                                   \
-        if (group == 2)                                                    \
-            k_count<F, K, 2><<<grid, kThreads, 0, st>>>(a);                \
-        else                                                               \
-            k_count<F, K, 4><<<grid, kThreads, 0, st>>>(a);                \
-    } while (0)
-#define NBL_GO_F(F, K) launch_fill<F, K>(a, grid, st)
-#define NBL_BY_KIND(GO, F)                            \
-    do {                                              \
-        if (kind == kCutPerAtom)                      \
-            GO(F, kCutPerAtom);                       \
-        else if (kind == kCutPerType)                 \
-            GO(F, kCutPerType);                       \
-        else                                          \
-            GO(F, kCutScalar);                        \
-    } while (0)
-    if (mode == kModeCount) {
-        if (fp32)
-            NBL_BY_KIND(NBL_GO_C, true);
-        else
-            NBL_BY_KIND(NBL_GO_C, false);
-    } else {
-        if (fp32)
-            NBL_BY_KIND(NBL_GO_F, true);
-        else
-            NBL_BY_KIND(NBL_GO_F, false);
-    }
-#undef NBL_BY_KIND
-#undef NBL_GO_C
-#undef NBL_GO_F
-    count_launch();
-    return cudaGetLastError();
+    if (!traverse_shape_ok(mode, fp32, shape)) return cudaErrorInvalidValue;
+    if (mode == kModeCount)
+        return fp32 ? launch_count_fp32(kind, a, grid, st, shape)
+                    : launch_count_fp64(kind, a, grid, st, shape);
+    return fp32 ? launch_fill_fp32(kind, a, grid, st, shape)
+                : launch_fill_fp64(kind, a, grid, st, shape);
 }
 
 }  // namespace nbl

@@ -104,6 +104,19 @@ struct TraverseArgs {
     // each warp claims its next item with one atomic, so warps that drew
     // cheap items take more.  NULL: a fixed warp stride over the items.
     int *item_next;
+    // Atoms per work item (the cell-occupancy tile, <= 32): the items were
+    // cut by k_tiles with the same value.
+    int itile;
+};
+
+// Launch shape of one pair pass: warps per CTA (2, 4 or 8, i.e. 64, 128 or
+// 256 threads), candidates staged per warp in the count (cand 0: 384 FP32 /
+// 192 FP64 positions, cand 1: 768 / 384), atoms swept together per pass in
+// the FP32 count (2 or 4).  A tuning choice with no effect on results.
+struct TravShape {
+    int warps = 4;
+    int cand = 0;
+    int group = 4;
 };
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
@@ -114,8 +127,6 @@ cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);
 // work item.
 constexpr int kMaskBatches = 4;
 
-// Warps per CTA of the pair passes (sizes per-warp partial arrays).
-constexpr int kTraverseWarps = 4;
 
 // Sum of n per-atom energies in a fixed order into *out (one double);
 // scratch holds at least n / 2048 + n / 2048^2 + 2 doubles.
@@ -124,15 +135,36 @@ cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, d
 
 // Fill the visit tables of the systems that have one (visit_base >= 0).
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
+// Work items: each occupied cell cut into tiles of `itile` (<= 32) atoms.
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         int2 *items, int *n_items, int64_t natoms, int num_sms,
+                         int2 *items, int *n_items, int64_t natoms, int num_sms, int itile,
                          cudaStream_t st);
-// group: atoms swept together per pass in the FP32 count (2 or 4).
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
-                            int grid, cudaStream_t st, int group = 4);
-// CTAs of the pair pass (mode, precision, cutoff kind, count group, force
-// sink) resident per SM on the current device: the grid of one full wave is
-// this times the SM count.  0 on error.
-int traverse_blocks_per_sm(int mode, bool fp32, int kind, int group = 4, bool lj = false);
+                            int grid, cudaStream_t st, const TravShape &shape = TravShape());
+// CTAs of the pair pass (mode, precision, cutoff kind, shape, force sink)
+// resident per SM on the current device: the grid of one full wave is this
+// times the SM count.  0 on error.
+int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape = TravShape(),
+                           bool lj = false);
+// Candidates one count warp stages per sweep for a shape.
+constexpr int count_candidates(bool fp32, int cand) {
+    return (fp32 ? 384 : 192) * (cand != 0 ? 2 : 1);
+}
+// Whether `shape` is one of the compiled launch shapes of the pass.
+bool traverse_shape_ok(int mode, bool fp32, const TravShape &shape);
+
+// Per precision and pass (nbl_trav_*.cu): launch / resident CTAs per SM.
+cudaError_t launch_count_fp32(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                              const TravShape &shape);
+cudaError_t launch_count_fp64(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                              const TravShape &shape);
+cudaError_t launch_fill_fp32(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                             const TravShape &shape);
+cudaError_t launch_fill_fp64(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                             const TravShape &shape);
+int occupancy_count_fp32(int kind, const TravShape &shape);
+int occupancy_count_fp64(int kind, const TravShape &shape);
+int occupancy_fill_fp32(int kind, const TravShape &shape, bool lj);
+int occupancy_fill_fp64(int kind, const TravShape &shape, bool lj);
 
 }  // namespace nbl

@@ -135,6 +135,18 @@ __device__ __forceinline__ bool raw_cell_of(const SysDev &S, const double *r,
     return ok;
 }
 
+// Offset vector of cell offset d (neighbour_visit.hh:67,73,80):
+// off3 = z b3; off2 = off3 + y b2; off = off2 + x b1, in FP64 without FMA.
+__device__ __forceinline__ void visit_offset(const SysDev &S, const int d[3], double o[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double v = dmul((double)d[2], S.bin[2][k]);
+        v = dadd(v, dmul((double)d[1], S.bin[1][k]));
+        v = dadd(v, dmul((double)d[0], S.bin[0][k]));
+        o[k] = v;
+    }
+}
+
 // 64-bit mixer for the hashed grid (splitmix64 finaliser).
 __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
     x ^= x >> 30;
@@ -143,6 +155,31 @@ __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long 
     x *= 0x94d049bb133111ebull;
     x ^= x >> 31;
     return x;
+}
+
+// Lanes below the calling lane.
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Slice of hashed cell `key`: open addressing with linear probing, at most
+// mask + 1 probes; an absent key gives an empty slice, a full table without
+// the key sets kErrInternal (never a wait).
+__device__ __forceinline__ int2 hash_find(const unsigned long long *__restrict__ hkey,
+                                          unsigned long long mask,
+                                          const int2 *__restrict__ table,
+                                          unsigned long long key, int *err) {
+    unsigned long long h = mix64(key) & mask;
+    for (unsigned long long p = 0; p <= mask; p++) {
+        unsigned long long cur = hkey[h];
+        if (cur == key) return table[h];
+        if (cur == kHashEmpty) return make_int2(0, 0);
+        h = (h + 1) & mask;
+    }
+    atomicOr(err, kErrInternal);
+    return make_int2(0, 0);
 }
 
 // Interleave the low 10 bits of three coordinates (Morton / Z-order key).

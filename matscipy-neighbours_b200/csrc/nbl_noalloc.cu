@@ -261,7 +261,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     NA_CUDA(launch_gather(ga, s), "k_gather");
     int nsm_tiles = 148;
     cudaDeviceGetAttribute(&nsm_tiles, cudaDevAttrMultiProcessorCount, dev);
-    NA_CUDA(launch_tiles(home, small, table, items, small + 3, N, nsm_tiles, s), "k_tiles");
+    NA_CUDA(launch_tiles(home, small, table, items, small + 3, N, nsm_tiles, 32, s), "k_tiles");
 
     TraverseArgs ta{};
     ta.sys = sys;
@@ -285,6 +285,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.item_next = small + 6;
     ta.i_lo = 0;
     ta.i_hi = INT64_MAX;
+    ta.itile = 32;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // two whole waves of each pass's resident CTAs

@@ -84,11 +84,15 @@ struct Plan {
     int trav_grid = 0;        // count-pass grid (CTAs)
     int fill_grid = 0;        // fill-pass grid (CTAs)
     // Launch configuration (set by the autotuner for batches, or by
-    // nbl_plan_set_launch): CTAs per SM of the count and fill passes (0: a
-    // whole number of waves of resident CTAs), atoms per sweep in the count.
+    // nbl_plan_set_launch / nbl_plan_set_launch_config): CTAs per SM of the
+    // count and fill passes (0: a whole number of waves of resident CTAs),
+    // each pass's launch shape (warps per CTA, staged candidates, atoms per
+    // sweep) and the atoms per work item (cell-occupancy tile).
     int count_mult = 0;
     int fill_mult = 0;
-    int count_group = 4;
+    TravShape count_shape;
+    TravShape fill_shape;
+    int itile = 32;
     // Work items by atomic ticket (else a fixed warp stride) in each pass.
     bool count_tickets = true;
     bool fill_tickets = true;
@@ -136,5 +140,6 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st);
 nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync);
 nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_t st);
 nbl_status read_flags(Plan &p, cudaStream_t st);
+void launch_config_of(const Plan &p, nbl_launch_config *cfg);
 
 }  // namespace nbl

@@ -69,6 +69,18 @@ class Outputs(ctypes.Structure):
                 ("shift", ctypes.c_void_p)]
 
 
+class LaunchConfig(ctypes.Structure):
+    """``nbl_launch_config`` (include/nbl_b200.h): the pair passes' launch
+    configuration (zero fields: defaults)."""
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "count_ctas_per_sm", "fill_ctas_per_sm", "count_strided", "fill_strided",
+        "count_warps", "fill_warps", "count_group", "count_large_staging",
+        "atoms_per_item")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 def _load():
     if not _LIB_PATH.exists():
         raise ImportError(
@@ -82,6 +94,9 @@ def _load():
         "nbl_plan_trim": ([P], ctypes.c_int),
         "nbl_set_atom_range": ([P, ctypes.c_int64, ctypes.c_int64], ctypes.c_int),
         "nbl_plan_set_launch": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "nbl_plan_set_launch_config": ([P, ctypes.POINTER(LaunchConfig)], ctypes.c_int),
+        "nbl_plan_get_launch_config": ([P, ctypes.POINTER(LaunchConfig)], ctypes.c_int),
+        "nbl_debug_inject": ([ctypes.c_int, ctypes.c_int64], ctypes.c_int),
         "nbl_count": ([P, ctypes.POINTER(Request), P, ctypes.POINTER(ctypes.c_int64)],
                       ctypes.c_int),
         "nbl_fill": ([P, ctypes.POINTER(Outputs), P], ctypes.c_int),

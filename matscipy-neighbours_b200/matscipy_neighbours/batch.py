@@ -58,6 +58,9 @@ def _sigs():
                                   ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "nbl_batch_get_tickets": ([P, ctypes.POINTER(ctypes.c_int),
                                    ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "nbl_batch_get_launch_config": ([P, ctypes.POINTER(_ext.LaunchConfig),
+                                         ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     }
     for name, (args, res) in table.items():
         fn = getattr(lib, name)
@@ -244,6 +247,24 @@ class NeighbourListBatch:
         _ext.check(self._lib.nbl_batch_get_config(self._h, ctypes.byref(a), ctypes.byref(b),
                                                   ctypes.byref(c)))
         return a.value, b.value, c.value
+
+    def launch_config(self):
+        """Everything the autotuner chose (``nbl_launch_config`` as a dict:
+        grids, work-item striding, warps per CTA of each pass, atoms per FP32
+        sweep, candidate staging, atoms per work item) plus the median
+        count-phase and fill times it measured for that choice (ms; 0 without
+        tuning)."""
+        cfg = _ext.LaunchConfig()
+        cms, fms = ctypes.c_float(), ctypes.c_float()
+        _ext.check(self._lib.nbl_batch_get_launch_config(self._h, ctypes.byref(cfg),
+                                                         ctypes.byref(cms), ctypes.byref(fms)))
+        out = cfg.as_dict()
+        fp32 = self._precision == _ext.PRECISION_FP32_FILTER
+        out["count_candidates_per_warp"] = (384 if fp32 else 192) * (
+            2 if out["count_large_staging"] else 1)
+        out["tuned_count_ms"] = float(cms.value)
+        out["tuned_fill_ms"] = float(fms.value)
+        return out
 
     def tickets(self):
         """(count pass, fill pass) hand out work items by atomic ticket."""

@@ -102,6 +102,12 @@ def test_batch_autotune_picks_a_config(oracle):
     # CTAs per SM: 1, 2 or 4 waves of each kernel's resident CTAs
     assert 1 <= cm <= 64 and grp in (2, 4) and 1 <= fm <= 64
     assert all(isinstance(t, bool) for t in b.tickets())
+    lc = b.launch_config()
+    assert lc["count_warps"] in (2, 4, 8) and lc["fill_warps"] in (2, 4, 8)
+    assert lc["atoms_per_item"] in (16, 32) and lc["count_large_staging"] in (0, 1)
+    assert lc["count_group"] == grp and lc["count_ctas_per_sm"] == cm
+    assert lc["count_candidates_per_warp"] in (384, 768)
+    assert lc["tuned_count_ms"] > 0 and lc["tuned_fill_ms"] > 0
     b.run()
     _check(oracle, b, systems)
     b.close()
