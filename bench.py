@@ -702,6 +702,55 @@ def cpu_baseline(steps=2, want=None):
     return out
 
 
+def reference_gpu_bench(dev, w, pos_d, outs, npairs, reps=5):
+    """The reference's own CUDA backend (oracle/_ref/libref_gpu.so: its
+    neighbour_list_gpu_device compiled for sm_100a from its sources) on the
+    same device-resident workload, as a secondary comparator: the device time
+    of its call (its own allocations, copies and synchronisations included),
+    median of `reps` after one warm-up; and its pairs against the engine's,
+    canonically ordered by (i, j) since its row order is not the reference
+    CPU's: the same (i, j, S) and the largest |D|, |d| differences."""
+    import torch
+    O = _oracle()
+    if not O.refgpu_available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (reference sources "
+                               "absent when build() ran)"}
+    nat = pos_d.shape[0]
+    ref = {"i": torch.empty(npairs, dtype=torch.int32, device=dev),
+           "j": torch.empty(npairs, dtype=torch.int32, device=dev),
+           "D": torch.empty((npairs, 3), dtype=torch.float64, device=dev),
+           "d": torch.empty(npairs, dtype=torch.float64, device=dev),
+           "S": torch.empty((npairs, 3), dtype=torch.int32, device=dev)}
+    torch.cuda.synchronize(dev)
+    n, _ = O.refgpu_neighbour_list("ijDdS", w["cell"], pos_d.data_ptr(), nat, w["cutoff"],
+                                   w["pbc"], outputs=[ref[q].data_ptr() for q in "ijDdS"],
+                                   capacity=npairs)
+    ms = []
+    for _ in range(reps):
+        _, t = O.refgpu_neighbour_list("ijdDS", w["cell"], pos_d.data_ptr(), nat, w["cutoff"],
+                                       w["pbc"])
+        ms.append(t)
+    out = {"what": "reference neighbour_list_gpu_device (its CUDA backend, sm_100a build)",
+           "npairs": n, "ms_per_build": statistics.median(ms),
+           "value": n / (statistics.median(ms) * 1e-3), "unit": UNIT}
+    if n == npairs:
+        def canon(o):
+            key = o["i"].to(torch.int64) * nat + o["j"].to(torch.int64)
+            order = torch.sort(key, stable=True).indices
+            return key[order], o["S"][order], o["D"][order], o["d"][order]
+        ka, sa, da, aa = canon(ref)
+        kb, sb, db, ab = canon(outs)
+        out["same_ij_S"] = bool(torch.equal(ka, kb) and torch.equal(sa, sb))
+        out["max_abs_diff_D"] = float((da - db).abs().max()) if npairs else 0.0
+        out["max_abs_diff_d"] = float((aa - ab).abs().max()) if npairs else 0.0
+        del ka, sa, da, aa, kb, sb, db, ab
+    else:
+        out["same_ij_S"] = False
+    del ref
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank):
     """The reference's own CPU core (oracle/_ref: its neighbour_list.cc and
     cell_list.cc compiled from source, OpenMP) on every host thread, on the
@@ -747,6 +796,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA backend")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the bit-for-bit comparisons with the CPU checker")
     ap.add_argument("--no-fp64", action="store_true")
@@ -962,6 +1013,13 @@ def main():
             def want(res):
                 parity["C2"] = _same_device("ijdDS", [outs[q] for q in "ijdDS"], res)
         out["cpu_baseline"] = cpu_baseline(want=want)
+    if world == 1 and not args.no_reference_gpu and args.reps == 64:
+        timed_steps(req, 1)
+        ext.check(ext.lib.nbl_check(plan, sptr))
+        rg = reference_gpu_bench(dev, w, pos_d, outs, npairs)
+        if "ms_per_build" in rg:
+            rg["engine_speedup"] = rg["ms_per_build"] / (total_ms / args.steps)
+        out["reference_gpu"] = rg
     if parity:
         out["parity"] = parity
         out["parity_checker"] = ("oracle/_ref (the reference's own CPU core, compiled from its "

@@ -34,6 +34,7 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libref_neighbours.so"
+REF_GPU_SO = HERE / "_ref" / "libref_gpu.so"
 
 _QBITS = {"i": 1, "j": 2, "D": 4, "d": 8, "S": 16}
 
@@ -79,6 +80,8 @@ def build():
     src = reference_src()
     if src.is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_SRC={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref_gpu", f"REF_SRC={src}"],
+                       check=True)
 
 
 def _load():
@@ -333,3 +336,41 @@ def ref_first_neighbours(n, i):
 def ref_triplet_list(first_i, absdist=None, cutoff=None):
     """The reference's own triplet_list (oracle/_ref)."""
     return _csr_triplets(_load_ref().ref_triplet_list, first_i, absdist, cutoff)
+
+
+# ---- the reference's CUDA backend (a timing comparator) ---------------------
+
+def refgpu_available():
+    return REF_GPU_SO.exists()
+
+
+def refgpu_neighbour_list(quantities, cell, positions_ptr, nat, cutoff, pbc=True, origin=None,
+                          outputs=None, capacity=0):
+    """One build by the reference's own CUDA backend (oracle/_ref/libref_gpu.so,
+    neighbour_list_gpu_device, src/libneighbours/neighbour_list_gpu.cc:518) of
+    device positions at `positions_ptr` (an integer device address, `nat`
+    atoms); scalar cutoff.  Returns (npairs, device milliseconds of the call).
+    `outputs` (five integer device addresses, in "ijDdS" order, or None)
+    receive the pairs when `capacity` holds them."""
+    lib = ctypes.CDLL(str(REF_GPU_SO))
+    fn = lib.refgpu_neighbour_list
+    P = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_int, P, ctypes.c_double,
+                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_float),
+                   P, P, P, P, P, ctypes.c_int64]
+    fn.restype = ctypes.c_int
+    cell = np.ascontiguousarray(cell, dtype=np.float64).reshape(3, 3)
+    inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+    origin = (np.zeros(3) if origin is None
+              else np.ascontiguousarray(origin, dtype=np.float64))
+    pb = np.ascontiguousarray(np.broadcast_to(pbc, (3,)), dtype=np.int32)
+    n = ctypes.c_int64()
+    ms = ctypes.c_float()
+    outs = outputs if outputs is not None else (None,) * 5
+    st = fn(_flags(quantities), _dptr(origin), _dptr(cell), _dptr(inv), _dptr(pb), int(nat),
+            ctypes.c_void_p(int(positions_ptr)), float(cutoff), ctypes.byref(n),
+            ctypes.byref(ms), *[None if o is None else ctypes.c_void_p(int(o)) for o in outs],
+            int(capacity))
+    if st != 0:
+        raise OracleError("reference GPU backend returned an error")
+    return int(n.value), float(ms.value)
