@@ -1,6 +1,8 @@
-"""ASE neighbour-list plugin entry point (the reference's
-``matscipy_neighbours._ase_plugin``, registered there under the
-``ase.plugins`` entry point, pyproject.toml:22-23).
+"""ASE neighbour-list adapter (the reference's ``matscipy_neighbours._ase_plugin``,
+which its packaging registers under the ``ase.plugins`` entry point,
+pyproject.toml:22-23).  This tree ships no packaging metadata, so ASE does not
+discover the module by itself: import it, or declare the entry point in the
+package that installs it.
 
 ``neighbor_list`` follows ASE's neighbour-list protocol: ``(quantities,
 atoms, cutoff, *, self_interaction=False)`` returning the flat ``i, j, d, D,
