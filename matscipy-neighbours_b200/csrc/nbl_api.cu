@@ -239,12 +239,14 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_pos = b.pos_on_device ? 0 : L.add(sizeof(double) * 3 * N);
     size_t o_pa = (b.per_atom && !b.aux_on_device) ? L.add(sizeof(double) * N) : 0;
     size_t o_ty = (b.types && !b.aux_on_device) ? L.add(sizeof(int32_t) * N) : 0;
+    // the small host tables, contiguous (one upload)
     size_t o_sys = L.add(sizeof(SysDev) * nsys);
-    const int64_t nvis = visit_entries(b);
-    size_t o_vis = nvis ? L.add(sizeof(VisitDev) * nvis) : 0;
     size_t o_sab = L.add(sizeof(int64_t) * nsys);
     size_t o_pt64 = L.add(sizeof(double) * std::max<size_t>(b.pt64.size(), 1));
     size_t o_pt32 = L.add(sizeof(float) * std::max<size_t>(b.pt64.size(), 1));
+    const size_t tab_end = L.total;
+    const int64_t nvis = visit_entries(b);
+    size_t o_vis = nvis ? L.add(sizeof(VisitDev) * nvis) : 0;
     size_t o_keys = L.add(sizeof(uint32_t) * N);
     size_t o_vals = L.add(sizeof(int32_t) * N);
     size_t o_keys2 = L.add(sizeof(uint32_t) * N);
@@ -261,13 +263,12 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     size_t o_amax = L.add(sizeof(float) * nsys);
     size_t o_home = L.add(sizeof(HomeCell) * N);
     size_t o_cnt = L.add(sizeof(int32_t) * (N + 1));
-    size_t o_off = L.add(sizeof(int64_t) * (N + 1));
-    size_t o_small = L.add(sizeof(int) * 8);  // n_home, err, overflow, items, mask cursor,
-                                              // item ticket
+    // row offsets, then the 8-int flag block right after offsets[N]
+    size_t o_off = L.add(sizeof(int64_t) * (N + 1) + sizeof(int) * 8);
     const int64_t mask_cap = mask_words(p, b);
     size_t o_mask = L.add(sizeof(uint32_t) * mask_cap);
     size_t o_hmask = L.add(sizeof(long long) * std::max<int64_t>(N, 1) * kMaskBatches);
-    size_t o_items = L.add(sizeof(int2) * std::max<int64_t>(N, 1));
+    size_t o_items = L.add(sizeof(WorkItem) * std::max<int64_t>(N, 1));
     size_t o_ljp = L.add(sizeof(double) * (size_t)(std::max<int64_t>(N, 1) + N / 1024 + 64));
     nbl_status st = ensure(p.ws.base, p.ws.bytes, L.total, "workspace");
     if (st != NBL_SUCCESS) {
@@ -285,6 +286,10 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
                                          : (int32_t *)at(o_ty))
                       : nullptr;
     B.sys = (SysDev *)at(o_sys);
+    B.tab_sab = o_sab - o_sys;
+    B.tab_pt64 = o_pt64 - o_sys;
+    B.tab_pt32 = o_pt32 - o_sys;
+    B.tab_bytes = tab_end - o_sys;
     B.visit = nvis ? (VisitDev *)at(o_vis) : nullptr;
     B.sys_atom_base = (int64_t *)at(o_sab);
     B.pt64 = (double *)at(o_pt64);
@@ -306,11 +311,11 @@ static nbl_status layout_workspace(Plan &p, const Batch &b) {
     B.home = (HomeCell *)at(o_home);
     B.counts = (int32_t *)at(o_cnt);
     B.offsets = (int64_t *)at(o_off);
-    B.small = (int *)at(o_small);
+    B.small = reinterpret_cast<int *>(B.offsets + N + 1);
     B.mask_pool = (uint32_t *)at(o_mask);
     B.mask_cap = mask_cap;
     B.home_mask = (long long *)at(o_hmask);
-    B.items = (int2 *)at(o_items);
+    B.items = (WorkItem *)at(o_items);
     B.lj_part = (double *)at(o_ljp);
     return NBL_SUCCESS;
 }
@@ -412,8 +417,7 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
     // Small host tables go through the plan's pinned staging so the copies
     // are truly asynchronous and the staging stays valid until they run.
     {
-        size_t need = sizeof(SysDev) * nsys + sizeof(int64_t) * nsys +
-                      (sizeof(double) + sizeof(float)) * b.pt64.size() + 64;
+        size_t need = B.tab_bytes + 64;
         if (need > p.host_stage_bytes) {
             if (p.host_stage) {
                 cudaStreamSynchronize(st);
@@ -427,6 +431,7 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
             // The previous call's staging copies must have run before reuse.
             NBL_CUDA(cudaEventSynchronize(p.stage_done), "staging reuse");
         }
+        // the same layout as the device block at B.sys: one copy
         char *h = static_cast<char *>(p.host_stage);
         std::memcpy(h, b.sys.data(), sizeof(SysDev) * nsys);
         if (B.visit != nullptr) {
@@ -437,25 +442,16 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
                 base += hs[s2].nvisit;
             }
         }
-        NBL_CUDA(cudaMemcpyAsync(B.sys, h, sizeof(SysDev) * nsys, cudaMemcpyHostToDevice, st),
-                 "copy systems");
-        h += sizeof(SysDev) * nsys;
-        int64_t *sab = reinterpret_cast<int64_t *>(h);
+        int64_t *sab = reinterpret_cast<int64_t *>(h + B.tab_sab);
         for (int s2 = 0; s2 < nsys; s2++) sab[s2] = b.sys[s2].atom_base;
-        NBL_CUDA(cudaMemcpyAsync(B.sys_atom_base, sab, sizeof(int64_t) * nsys,
-                                 cudaMemcpyHostToDevice, st), "copy systems");
-        h += sizeof(int64_t) * nsys;
         if (!b.pt64.empty()) {
-            double *p64 = reinterpret_cast<double *>(h);
+            double *p64 = reinterpret_cast<double *>(h + B.tab_pt64);
             std::memcpy(p64, b.pt64.data(), sizeof(double) * b.pt64.size());
-            h += sizeof(double) * b.pt64.size();
-            float *p32 = reinterpret_cast<float *>(h);
+            float *p32 = reinterpret_cast<float *>(h + B.tab_pt32);
             for (size_t k = 0; k < b.pt64.size(); k++) p32[k] = (float)b.pt64[k];
-            NBL_CUDA(cudaMemcpyAsync(B.pt64, p64, sizeof(double) * b.pt64.size(),
-                                     cudaMemcpyHostToDevice, st), "copy per-type cutoffs");
-            NBL_CUDA(cudaMemcpyAsync(B.pt32, p32, sizeof(float) * b.pt64.size(),
-                                     cudaMemcpyHostToDevice, st), "copy per-type cutoffs");
         }
+        NBL_CUDA(cudaMemcpyAsync(B.sys, h, B.tab_bytes, cudaMemcpyHostToDevice, st),
+                 "copy systems");
         NBL_CUDA(cudaEventRecord(p.stage_done, st), "staging event");
         p.stage_in_flight = true;
     }
@@ -470,12 +466,9 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     Bufs &B = p.bufs;
     const int64_t N = b.natoms;
     const int nsys = (int)b.sys.size();
-    NBL_CUDA(cudaMemsetAsync(B.small, 0, sizeof(int) * 8, st), "memset");
-    NBL_CUDA(cudaMemsetAsync(B.table, 0, sizeof(int2) * b.table_size, st), "memset table");
-    if (b.grid == kGridHashed)
-        NBL_CUDA(cudaMemsetAsync(B.hkey, 0xff, sizeof(unsigned long long) * b.table_size, st),
-                 "memset hash");
-    NBL_CUDA(cudaMemsetAsync(B.amax, 0, sizeof(float) * nsys, st), "memset");
+    NBL_CUDA(launch_init(B.sys, nsys, B.visit, B.small, B.table, b.table_size, B.amax,
+                         b.grid == kGridHashed ? B.hkey : nullptr, p.num_sms, st),
+             "k_init");
 
     int *n_home = B.small + 0;
     int *err = B.small + 1;
@@ -531,7 +524,6 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
         NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms,
                               p.itile, st),
                  "k_tiles");
-        NBL_CUDA(launch_visit(B.sys, nsys, B.visit, st), "k_visit");
     }
 
     TraverseArgs &ta = p.targs;
@@ -572,7 +564,9 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
                                 p.fill_shape, false);
     {
         StageRange r("nbl.count");
-        NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, ta, p.trav_grid, st,
+        TraverseArgs tc = ta;
+        tc.ticket_ready = 1;  // k_init cleared the ticket
+        NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, tc, p.trav_grid, st,
                                  p.count_shape),
                  "count pass");
     }
@@ -591,10 +585,9 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     Bufs &B = p.bufs;
     const int64_t N = b.natoms;
     if (sync) {
-        NBL_CUDA(cudaMemcpyAsync(p.host_small, B.offsets + N, sizeof(int64_t),
-                                 cudaMemcpyDeviceToHost, st), "read pair count");
-        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, B.small, sizeof(int) * 6,
-                                 cudaMemcpyDeviceToHost, st), "read flags");
+        // pair count and flags in one copy (the flag block follows offsets[N])
+        NBL_CUDA(cudaMemcpyAsync(p.host_small, B.offsets + N, sizeof(int64_t) + sizeof(int) * 6,
+                                 cudaMemcpyDeviceToHost, st), "read pair count and flags");
         NBL_CUDA(cudaStreamSynchronize(st), "count phase");
         p.stage_in_flight = false;
         int flags[6];

@@ -509,10 +509,9 @@ NBL_API nbl_status nbl_batch_setup(nbl_batch *bt, const nbl_batch_request *req,
     if (capacity <= 0) {
         s = enqueue_count(bt->p, b, st);
         if (s != NBL_SUCCESS) return s;
-        NBL_CUDA(cudaMemcpyAsync(bt->p.host_small, bt->p.bufs.offsets + N, sizeof(int64_t),
-                                 cudaMemcpyDeviceToHost, st), "read pair count");
-        NBL_CUDA(cudaMemcpyAsync(bt->p.host_small + 1, bt->p.bufs.small, sizeof(int) * 6,
-                                 cudaMemcpyDeviceToHost, st), "read mask demand");
+        NBL_CUDA(cudaMemcpyAsync(bt->p.host_small, bt->p.bufs.offsets + N,
+                                 sizeof(int64_t) + sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
+                 "read pair count and mask demand");
         NBL_CUDA(cudaStreamSynchronize(st), "count");
         capacity = bt->p.host_small[0] + bt->p.host_small[0] / 4 + 4096;
         // More hit words asked for than the estimate held: re-plan the
@@ -619,10 +618,9 @@ NBL_API nbl_status nbl_batch_finish(nbl_batch *bt, void *stream, int64_t *npairs
     Guard g(bt->p.device);
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : bt->own_stream;
     const int64_t N = bt->b.natoms;
-    NBL_CUDA(cudaMemcpyAsync(bt->p.host_small, bt->p.bufs.offsets + N, sizeof(int64_t),
-                             cudaMemcpyDeviceToHost, st), "read pair count");
-    NBL_CUDA(cudaMemcpyAsync(bt->p.host_small + 1, bt->p.bufs.small, sizeof(int) * 2,
-                             cudaMemcpyDeviceToHost, st), "read flags");
+    NBL_CUDA(cudaMemcpyAsync(bt->p.host_small, bt->p.bufs.offsets + N,
+                             sizeof(int64_t) + sizeof(int) * 2, cudaMemcpyDeviceToHost, st),
+             "read pair count and flags");
     NBL_CUDA(cudaStreamSynchronize(st), "batch");
     int flags[2];
     std::memcpy(flags, bt->p.host_small + 1, sizeof(flags));

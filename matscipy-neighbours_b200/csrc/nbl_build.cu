@@ -216,7 +216,7 @@ k_gather(GatherArgs a) {
 // small periodic system often is one cell) while the rest of the GPU idles.
 __global__ void __launch_bounds__(256)
 k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
-        const int2 *__restrict__ table, int2 *__restrict__ items, int *__restrict__ n_items,
+        const int2 *__restrict__ table, WorkItem *__restrict__ items, int *__restrict__ n_items,
         int itile) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -224,7 +224,11 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
     for (int base = blockIdx.x * blockDim.x; base < nh; base += gridDim.x * blockDim.x) {
         const int h = base + threadIdx.x;
         int2 hs = make_int2(0, 0);
-        if (h < nh) hs = table[home[h].tidx];
+        HomeCell hc{};
+        if (h < nh) {
+            hc = home[h];
+            hs = table[hc.tidx];
+        }
         const int nt = (hs.y - hs.x + itile - 1) / itile;
         int incl = nt;
 #pragma unroll
@@ -236,12 +240,23 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
         int first = 0;
         if (lane == 0 && tot > 0) first = atomicAdd(n_items, tot);
         first = __shfl_sync(full, first, 0) + incl - nt;
-        for (int t = 0; t < nt; t++) items[first + t] = make_int2(h, hs.x + itile * t);
+        for (int t = 0; t < nt; t++) {
+            WorkItem w;
+            w.c[0] = hc.c[0];
+            w.c[1] = hc.c[1];
+            w.c[2] = hc.c[2];
+            w.sys = hc.sys;
+            w.ib = hs.x + itile * t;
+            w.nt = min(itile, hs.y - w.ib);
+            w.tidx = hc.tidx;
+            w.pad = 0;
+            items[first + t] = w;
+        }
     }
 }
 
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         int2 *items, int *n_items, int64_t natoms, int num_sms, int itile,
+                         WorkItem *items, int *n_items, int64_t natoms, int num_sms, int itile,
                          cudaStream_t st) {
     if (natoms <= 0) return cudaSuccess;
     if (itile < 1 || itile > 32) return cudaErrorInvalidValue;
@@ -274,6 +289,54 @@ __global__ void k_visit(const SysDev *__restrict__ sys, VisitDev *__restrict__ v
         }
         visit[S.visit_base + v] = e;
     }
+}
+
+__global__ void __launch_bounds__(256)
+k_init(const SysDev *__restrict__ sys, int nsys, VisitDev *__restrict__ visit,
+       int *__restrict__ small, int2 *__restrict__ table, int64_t ntable,
+       float *__restrict__ amax, unsigned long long *__restrict__ hkey) {
+    if (visit != nullptr && (int)blockIdx.x < nsys) {
+        const SysDev &S = sys[blockIdx.x];
+        if (S.visit_base >= 0) {
+            const int nx = S.nscan[0], ny = S.nscan[1], nz = S.nscan[2];
+            const int wx = 2 * nx + 1, wy = 2 * ny + 1;
+            for (int v = threadIdx.x; v < S.nvisit; v += blockDim.x) {
+                const int xr = v % wx, rest = v / wx;
+                const int yr = rest % wy, zr = rest / wy;
+                const int d[3] = {xr - nx, yr - ny, zr - nz};
+                double o[3];
+                visit_offset(S, d, o);
+                VisitDev e;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    e.off[k] = o[k];
+                    e.off32[k] = __double2float_rn(o[k]);
+                    e.d[k] = d[k];
+                }
+                visit[S.visit_base + v] = e;
+            }
+        }
+    }
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    if (t0 < 8) small[t0] = 0;
+    for (int64_t i = t0; i < ntable; i += step) {
+        table[i] = make_int2(0, 0);
+        if (hkey != nullptr) hkey[i] = kHashEmpty;
+    }
+    for (int64_t i = t0; i < nsys; i += step) amax[i] = 0.f;
+}
+
+cudaError_t launch_init(const SysDev *sys, int nsys, VisitDev *visit, int *small, int2 *table,
+                        int64_t ntable, float *amax, unsigned long long *hkey, int num_sms,
+                        cudaStream_t st) {
+    const int64_t work = std::max<int64_t>(ntable, nsys);
+    int64_t blocks = std::min<int64_t>((work + 255) / 256, (int64_t)num_sms * 8);
+    blocks = std::max<int64_t>(blocks, visit != nullptr ? nsys : 1);
+    blocks = std::max<int64_t>(blocks, 1);
+    k_init<<<(unsigned)blocks, 256, 0, st>>>(sys, nsys, visit, small, table, ntable, amax, hkey);
+    count_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st) {

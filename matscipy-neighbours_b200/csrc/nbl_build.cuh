@@ -51,7 +51,7 @@ struct TraverseArgs {
     const VisitDev *visit;    // per-system visit tables (systems with visit_base >= 0)
     const HomeCell *home;
     const int *n_home;
-    const int2 *items;        // work items: (home cell, first atom of the i-tile)
+    const WorkItem *items;    // work items: (home cell, tile of its sorted atoms)
     const int *n_items;
     int grid;
     const int2 *table;
@@ -107,6 +107,9 @@ struct TraverseArgs {
     // Atoms per work item (the cell-occupancy tile, <= 32): the items were
     // cut by k_tiles with the same value.
     int itile;
+    // Nonzero: *item_next is already zero (the count phase's init kernel
+    // cleared it), so the launch skips its reset.
+    int ticket_ready;
 };
 
 // Launch shape of one pair pass: warps per CTA (2, 4 or 8, i.e. 64, 128 or
@@ -135,9 +138,15 @@ cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, d
 
 // Fill the visit tables of the systems that have one (visit_base >= 0).
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
+// Start of a count phase in one launch: zero the 8-int flag block, the cell
+// table (ntable int2) and the per-system maxima, mark every hash slot empty
+// (hkey != NULL), and fill the systems' visit tables (visit != NULL).
+cudaError_t launch_init(const SysDev *sys, int nsys, VisitDev *visit, int *small, int2 *table,
+                        int64_t ntable, float *amax, unsigned long long *hkey, int num_sms,
+                        cudaStream_t st);
 // Work items: each occupied cell cut into tiles of `itile` (<= 32) atoms.
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         int2 *items, int *n_items, int64_t natoms, int num_sms, int itile,
+                         WorkItem *items, int *n_items, int64_t natoms, int num_sms, int itile,
                          cudaStream_t st);
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, const TravShape &shape = TravShape());

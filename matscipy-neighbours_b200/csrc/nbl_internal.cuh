@@ -85,6 +85,47 @@ struct HomeCell {
     int32_t pad;
 };
 
+// One work item of the pair passes, self-contained so that a warp needs one
+// 32-byte load to start it: the home cell (folded coordinates, system) and
+// the tile of its sorted atoms [ib, ib + nt).
+struct __align__(16) WorkItem {
+    int32_t c[3];
+    int32_t sys;
+    int32_t ib;
+    int32_t nt;
+    int32_t tidx;
+    int32_t pad;
+};
+
+// Mask-pool reference of one (work item, segment batch), as the count stores
+// it: the first word in the low 40 bits, the batch's 32-candidate chunks per
+// atom above them; -1 when the item's words are not in the pool.
+constexpr int kMaskBaseBits = 40;
+__host__ __device__ __forceinline__ long long mask_ref(long long base, int nchunks) {
+    return base | ((long long)nchunks << kMaskBaseBits);
+}
+__host__ __device__ __forceinline__ long long mask_ref_base(long long ref) {
+    return ref < 0 ? -1ll : (ref & ((1ll << kMaskBaseBits) - 1));
+}
+__host__ __device__ __forceinline__ int mask_ref_chunks(long long ref) {
+    return ref < 0 ? 0 : (int)(ref >> kMaskBaseBits);
+}
+
+// Asynchronous global -> shared copies (cp.async, sm_80 and later): the data
+// lands in shared memory while the warp goes on; cp_async_wait waits for all
+// of the calling thread's copies (then __syncwarp before other lanes read).
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // Kernel launches issued by the calling host thread (reported through
 // nbl_launch_count()); every launch site bumps it.
 void count_launch(int n = 1);

@@ -179,7 +179,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     int32_t *counts = c.take<int32_t>(N + 1);
     int64_t *offsets = c.take<int64_t>(N + 1);
     int *small = c.take<int>(8);
-    int2 *items = c.take<int2>(std::max<int64_t>(N, 1));
+    WorkItem *items = c.take<WorkItem>(std::max<int64_t>(N, 1));
     if (!c.ok)
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "nbl_neighbour_list_noalloc: the request needs more than the "

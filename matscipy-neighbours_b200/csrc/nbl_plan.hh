@@ -56,11 +56,18 @@ struct Bufs {
     int64_t *offsets = nullptr;
     int *small = nullptr;  // [0] occupied cells, [1] error bits, [2] matrix
                            // overflow, [3] work items, [4..5] mask-pool cursor
-                           // (u64), [6] work-item ticket of the pair passes
+                           // (u64), [6] work-item ticket of the pair passes;
+                           // placed right after offsets[N], so one copy of
+                           // 32 bytes from offsets + N returns the pair count
+                           // and the first six flags
+    // The small host tables (systems, their atom bases, per-type cutoffs in
+    // FP64 and FP32) lie at these byte offsets from `sys`, one contiguous
+    // block of tab_bytes, so that they go up in one copy.
+    size_t tab_sab = 0, tab_pt64 = 0, tab_pt32 = 0, tab_bytes = 0;
     uint32_t *mask_pool = nullptr;
     long long mask_cap = 0;
     long long *home_mask = nullptr;
-    int2 *items = nullptr;
+    WorkItem *items = nullptr;
     double *lj_part = nullptr;     // force sink: per-atom energies, then block sums
 };
 

@@ -133,24 +133,26 @@ struct Hot {
 };
 
 struct Home {
-    HomeCell hc;
+    int32_t cc[3];  // folded coordinates of the home cell
+    int sys;
     const SysDev *S;
-    int2 hs;
     Hot H;
     int nvisit;
 };
 
 template <bool FP32>
-__device__ __forceinline__ Home load_home(const TraverseArgs &a, int h) {
+__device__ __forceinline__ Home load_home(const TraverseArgs &a, const WorkItem &w) {
     Home c;
-    c.hc = a.home[h];
-    c.S = a.sys + c.hc.sys;
+    c.cc[0] = w.c[0];
+    c.cc[1] = w.c[1];
+    c.cc[2] = w.c[2];
+    c.sys = w.sys;
+    c.S = a.sys + w.sys;
     const SysDev &S = *c.S;
-    c.hs = a.table[c.hc.tidx];
     c.H.lo_rc = c.H.hi_rc = c.H.band = 0.f;
     if (FP32) {
         const double R = S.cutoff;
-        const double M = 2.0 * (double)a.amax[c.hc.sys] + S.off_max;
+        const double M = 2.0 * (double)a.amax[w.sys] + S.off_max;
         const double band = guard_band(M, R);
         c.H.lo_rc = __double2float_rd(S.cutoff_sq - band);
         c.H.hi_rc = __double2float_ru(S.cutoff_sq + band);
@@ -216,7 +218,7 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         bool ok = true;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            int32_t x = c.hc.c[k] + off3[k];
+            int32_t x = c.cc[k] + off3[k];
             m[k] = 0;
             if (S.pbc[k]) {
                 const int32_t n = S.n[k];
@@ -236,7 +238,7 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
             cj[k] = x;
         }
         int2 sl = make_int2(0, 0);
-        if (ok) sl = cell_lookup(a, S, c.hc.sys, cj[0], cj[1], cj[2]);
+        if (ok) sl = cell_lookup(a, S, c.sys, cj[0], cj[1], cj[2]);
         len = sl.y - sl.x;
         sg.b[lane] = sl.x;
 #pragma unroll
@@ -424,11 +426,55 @@ __device__ __forceinline__ int first_item(const TraverseArgs &a, int gwarp, int 
     return __shfl_sync(0xffffffffu, t, 0);
 }
 
-// The warp's next work item: lane 0's ticket `pend` (claimed at the start of
-// the current item), else a fixed stride.
-__device__ __forceinline__ int next_item(const TraverseArgs &a, int it, int nwarps, int pend) {
-    if (a.item_next == nullptr) return it + nwarps;
-    return __shfl_sync(0xffffffffu, pend, 0);
+// A warp's walk over the work items, in ticket order (one atomic per item,
+// claimed one item ahead of its use) or at a fixed warp stride.  While the
+// current item runs, the record of the next one (and, for the fill, its first
+// mask-pool reference) is already on its way:
+//     ItemLoop L(...);
+//     while (L.it < nitems) { L.prefetch(...); <item L.it, L.rec, L.hm>; L.step(); }
+struct ItemLoop {
+    int it, nit;
+    int tk;                 // lane 0: the ticket after nit
+    WorkItem rec, nrec;
+    long long hm, nhm;      // first mask reference of it / nit (-1: none)
+
+    __device__ ItemLoop(const TraverseArgs &a, int gwarp, int nitems, int lane, bool want_hm) {
+        it = first_item(a, gwarp, lane);
+        tk = 0;
+        if (a.item_next != nullptr && lane == 0) tk = atomicAdd(a.item_next, 1);
+        nit = 0;
+        hm = nhm = -1;
+        if (it < nitems) {
+            rec = a.items[it];
+            if (want_hm && a.mask_pool != nullptr)
+                hm = a.home_mask[(long long)it * kMaskBatches];
+        }
+    }
+    __device__ void prefetch(const TraverseArgs &a, int nwarps, int nitems, int lane,
+                             bool want_hm) {
+        if (a.item_next != nullptr) {
+            nit = __shfl_sync(0xffffffffu, tk, 0);
+            if (lane == 0) tk = atomicAdd(a.item_next, 1);
+        } else {
+            nit = it + nwarps;
+        }
+        nhm = -1;
+        if (nit < nitems) {
+            nrec = a.items[nit];
+            if (want_hm && a.mask_pool != nullptr)
+                nhm = a.home_mask[(long long)nit * kMaskBatches];
+        }
+    }
+    __device__ void step() {
+        it = nit;
+        rec = nrec;
+        hm = nhm;
+    }
+};
+
+// Whether every atom produces rows (no nbl_set_atom_range split).
+__device__ __forceinline__ bool all_rows_of(const TraverseArgs &a) {
+    return a.i_lo <= 0 && a.i_hi >= (1ll << 40);
 }
 
 // Position of the (r+1)-th set bit of w (r < popc(w)).
@@ -472,23 +518,32 @@ k_count(TraverseArgs a) {
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    int pend = 0;  // lane 0: the ticket claimed while the current item runs
-    for (int it = first_item(a, gwarp, lane); it < nitems;
-         it = next_item(a, it, nwarps, pend)) {
-        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
-        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
-        const Home c = load_home<FP32>(a, item.x);
+    const bool all_rows = all_rows_of(a);
+    ItemLoop L(a, gwarp, nitems, lane, false);
+    while (L.it < nitems) {
+        L.prefetch(a, nwarps, nitems, lane, false);
+        const int it = L.it;
+        const Home c = load_home<FP32>(a, L.rec);
         const Hot &H = c.H;
-        const int2 hs = c.hs;
         long long mbase = -1;
 
-        {
-            const int ib = item.y;
+        do {
+            const int ib = L.rec.ib;
             // The tile's atoms whose original index lies in [i_lo, i_hi),
-            // compacted in order (all of them unless the rows are split).
+            // compacted in order (all of them unless the rows are split); with
+            // all rows they are copied asynchronously and land during the
+            // segment set-up.
             int ni;
-            {
-                const int nt = min(a.itile, hs.y - ib);
+            if (all_rows) {
+                ni = L.rec.nt;
+                if (lane < ni) {
+                    cp_async16(&sm.i32[lane], &a.pos32[ib + lane]);
+                    cp_async4(&sm.iatom[lane], &a.aux[ib + lane].x);
+                    sm.isi[lane] = ib + lane;
+                    sm.icount[lane] = 0;
+                }
+            } else {
+                const int nt = L.rec.nt;
                 int ax = 0;
                 bool in = false;
                 if (lane < nt) {
@@ -506,10 +561,12 @@ k_count(TraverseArgs a) {
                 }
                 __syncwarp();
             }
-            if (ni == 0) continue;
+            if (ni == 0) break;
             for (int vb = 0; vb < c.nvisit; vb += kSeg) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
+                cp_async_wait();
+                __syncwarp();
                 const int nchunks_all = (total + 31) >> 5;
                 // One word region per (work item, segment batch): (atoms of the
                 // i-tile) x (chunks of the batch's candidate list).
@@ -523,7 +580,9 @@ k_count(TraverseArgs a) {
                         if ((long long)b + words <= a.mask_cap) base = (long long)b;
                     }
                     base = __shfl_sync(full, base, 0);
-                    if (lane == 0) a.home_mask[(long long)it * kMaskBatches + vb / kSeg] = base;
+                    if (lane == 0)
+                        a.home_mask[(long long)it * kMaskBatches + vb / kSeg] =
+                            base >= 0 ? mask_ref(base, nchunks_all) : -1ll;
                     mbase = base;
                 }
                 // candidate index of atom si itself at offset 0 is kself0 + si
@@ -661,7 +720,8 @@ k_count(TraverseArgs a) {
             }
             if (lane < ni) a.counts[sm.iatom[lane]] = sm.icount[lane];
             __syncwarp();
-        }
+        } while (0);
+        L.step();
     }
 }
 
@@ -840,20 +900,36 @@ k_fill(TraverseArgs a) {
     const int nitems = *a.n_items;
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
-    int pend = 0;  // lane 0: the ticket claimed while the current item runs
-    for (int it = first_item(a, gwarp, lane); it < nitems;
-         it = next_item(a, it, nwarps, pend)) {
-        if (a.item_next != nullptr && lane == 0) pend = atomicAdd(a.item_next, 1);
-        const int2 item = a.items[it];  // (home cell, first atom of the i-tile)
-        const Home c = load_home<FP32>(a, item.x);
+    const bool all_rows = all_rows_of(a);
+    ItemLoop L(a, gwarp, nitems, lane, true);
+    while (L.it < nitems) {
+        L.prefetch(a, nwarps, nitems, lane, true);
+        const int it = L.it;
+        const Home c = load_home<FP32>(a, L.rec);
         const Hot &H = c.H;
-        const int2 hs = c.hs;
 
-        {
-            const int ib = item.y;
+        do {
+            const int ib = L.rec.ib;
             int ni;
-            {
-                const int nt = min(a.itile, hs.y - ib);
+            // The tile's atoms: with all rows copied asynchronously (they land
+            // during the segment set-up; the row starts follow once their
+            // indices are in), else the in-range ones compacted in order.
+            long long my_off = 0;
+            bool off_pending = false;
+            if (all_rows) {
+                ni = L.rec.nt;
+                if (lane < ni) {
+                    const char *src = reinterpret_cast<const char *>(a.pos64 + ib + lane);
+                    char *dst = reinterpret_cast<char *>(&sm.i64[lane]);
+                    cp_async16(dst, src);
+                    cp_async16(dst + 16, src + 16);
+                    cp_async16(&sm.iaux[lane], &a.aux[ib + lane]);
+                    sm.isi[lane] = ib + lane;
+                    if (LJ) facc[lane][0] = facc[lane][1] = facc[lane][2] = facc[lane][3] = 0.0;
+                }
+                off_pending = true;
+            } else {
+                const int nt = L.rec.nt;
                 int4 ax = make_int4(0, 0, 0, 0);
                 bool in = false;
                 if (lane < nt) {
@@ -873,14 +949,28 @@ k_fill(TraverseArgs a) {
                 }
                 __syncwarp();
             }
-            if (ni == 0) continue;
+            if (ni == 0) break;
+            // The first segment batch's hit words, when one window holds them
+            // all (the usual case), are copied asynchronously too.
+            const long long mb0 = mask_ref_base(L.hm);
+            const int nch0 = mask_ref_chunks(L.hm);
+            const bool words0 =
+                mb0 >= 0 && c.nvisit <= kSeg && ni * nch0 <= kWinWords && nch0 * 32 <= kRange;
+            if (words0)
+                for (int w = lane; w < ni * nch0; w += 32) cp_async4(&sm.mw[w], &a.mask_pool[mb0 + w]);
             for (int vb = 0; vb < c.nvisit; vb += kSeg) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
+                if (vb == 0) {
+                    cp_async_wait();
+                    __syncwarp();
+                    if (off_pending && lane < ni) my_off = (long long)a.offsets[sm.iaux[lane].x];
+                }
                 const int nchunks = (total + 31) >> 5;
                 const long long mbase =
                     (a.mask_pool != nullptr && vb / kSeg < kMaskBatches)
-                        ? a.home_mask[(long long)it * kMaskBatches + vb / kSeg]
+                        ? mask_ref_base(vb == 0 ? L.hm
+                                                : a.home_mask[(long long)it * kMaskBatches + vb / kSeg])
                         : -1ll;
                 // segment of each tabled candidate: lane = segment
                 if (lane < nseg) {
@@ -899,7 +989,10 @@ k_fill(TraverseArgs a) {
                         int na = min(win, ni - a0);
                         int nw = na * nch;
                         // --- the window's hit words ---------------------------------
-                        if (mbase >= 0) {
+                        if (mbase >= 0 && vb == 0 && kr == 0 && a0 == 0 && words0 &&
+                            nch0 == nchunks) {
+                            // already in shared memory (copied at the item's start)
+                        } else if (mbase >= 0) {
                             for (int w = lane; w < nw; w += 32) {
                                 const int al = div_small(w, nch, inv_nch);
                                 sm.mw[w] = a.mask_pool[mbase + (long long)(a0 + al) * nchunks +
@@ -951,6 +1044,11 @@ k_fill(TraverseArgs a) {
                             nw = na * nch;
                             carry = sm.mpre[nw];
                         }
+                        if (off_pending) {  // the row starts loaded after the tile landed
+                            if (lane < ni) sm.icur[lane] = my_off;
+                            off_pending = false;
+                            __syncwarp();
+                        }
                         // per-atom output base: slot = abase[atom] + window position
                         if (lane < na) sm.abase[lane] = sm.icur[a0 + lane] - sm.mpre[lane * nch];
                         __syncwarp();
@@ -995,6 +1093,10 @@ k_fill(TraverseArgs a) {
                     }
                 }
             }
+            if (off_pending) {  // no window ran (no candidates)
+                if (lane < ni) sm.icur[lane] = my_off;
+                __syncwarp();
+            }
             // --- fill must land exactly on the next row; matrix row lengths --------
             if (lane < ni) {
                 const int ax = sm.iaux[lane].x;
@@ -1013,7 +1115,8 @@ k_fill(TraverseArgs a) {
                 }
             }
             __syncwarp();
-        }
+        } while (0);
+        L.step();
     }
 }
 
@@ -1052,7 +1155,7 @@ inline cudaError_t launch_kernel(TravKernel kern, size_t smem, int warps, const 
                                  int grid, cudaStream_t st) {
     cudaError_t e = prepare_kernel(kern, smem);
     if (e != cudaSuccess) return e;
-    if (a.item_next != nullptr) {
+    if (a.item_next != nullptr && !a.ticket_ready) {
         e = cudaMemsetAsync(a.item_next, 0, sizeof(int), st);
         if (e != cudaSuccess) return e;
     }
