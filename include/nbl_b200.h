@@ -160,7 +160,8 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
      count_strided, fill_strided          work items by a fixed warp stride
                                           (1) instead of by atomic ticket (0)
      count_warps, fill_warps              block size: 2, 4 or 8 warps
-                                          (64, 128 or 256 threads; default 4)
+                                          (64, 128 or 256 threads; default
+                                          4 for the count, 8 for the fill)
      count_group                          atoms per FP32 sweep: 2 or 4 (4)
      count_large_staging                  candidates staged per count warp:
                                           0 = 384 (FP32) / 192 (FP64),

@@ -555,6 +555,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.i_lo = p.i_lo;
     ta.i_hi = p.i_hi;
     ta.itile = p.itile;
+    ta.natoms = N;
     if (p.i_lo > 0 || p.i_hi < N)
         NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
@@ -577,11 +578,112 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     return NBL_SUCCESS;
 }
 
+void drop_count_graph(Plan &p) {
+    if (p.count_graph) cudaGraphExecDestroy(p.count_graph);
+    p.count_graph = nullptr;
+    p.have_last_key = false;
+}
+
+static CountKey count_key(const Plan &p, const Batch &b) {
+    CountKey k;
+    k.ws_base = p.ws.base;
+    k.pos = p.bufs.pos;
+    k.per_atom = p.bufs.per_atom;
+    k.types = p.bufs.types;
+    k.natoms = b.natoms;
+    k.table_size = b.table_size;
+    k.mask_cap = p.bufs.mask_cap;
+    k.pt_size = (int64_t)b.pt64.size();
+    k.i_lo = p.i_lo;
+    k.i_hi = p.i_hi;
+    k.nsys = (int32_t)b.sys.size();
+    k.grid = b.grid;
+    k.key_bits = b.key_bits;
+    k.fp32 = b.fp32 ? 1 : 0;
+    k.kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
+    k.itile = p.itile;
+    k.nvisit_tab = p.bufs.visit != nullptr ? 1 : 0;
+    k.count_mult = p.count_mult;
+    k.count_warps = p.count_shape.warps;
+    k.count_cand = p.count_shape.cand;
+    k.count_group = p.count_shape.group;
+    k.count_tickets = p.count_tickets ? 1 : 0;
+    return k;
+}
+
+// Captures the count phase into p.count_graph (on the plan's own stream; the
+// capture runs nothing).  False if the capture fails: direct launches then.
+static bool capture_count(Plan &p, const Batch &b, const CountKey &k) {
+    if (!p.capture_stream &&
+        cudaStreamCreateWithFlags(&p.capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const long long before = g_launches;
+    if (cudaStreamBeginCapture(p.capture_stream, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const nbl_status s = enqueue_count(p, b, p.capture_stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(p.capture_stream, &g);
+    if (s != NBL_SUCCESS || e != cudaSuccess || g == nullptr) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return false;
+    }
+    if (p.count_graph) cudaGraphExecDestroy(p.count_graph);
+    p.count_graph = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&p.count_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        p.count_graph = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    p.graph_launches = g_launches - before;
+    count_launch((int)-p.graph_launches);  // nothing ran yet: counted at each replay
+    p.graph_key = k;
+    p.graph_targs = p.targs;
+    p.graph_trav_grid = p.trav_grid;
+    p.graph_kind = p.batch_kind;
+    return true;
+}
+
 nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     nbl_status s = upload_batch(p, b, st);
     if (s != NBL_SUCCESS) return s;
-    s = enqueue_count(p, b, st);
-    if (s != NBL_SUCCESS) return s;
+    // Single calls: replay the captured count phase while the launch key
+    // repeats (captured on the second call with the same key).
+    bool replay = false;
+    if (sync && !p.graphs_off) {
+        const CountKey k = count_key(p, b);
+        if (p.count_graph && k == p.graph_key) {
+            replay = true;
+        } else if (p.have_last_key && k == p.last_key) {
+            replay = capture_count(p, b, k);
+            if (!replay) {
+                p.graphs_off = true;
+                drop_count_graph(p);
+            }
+        }
+        p.last_key = k;
+        p.have_last_key = true;
+    }
+    if (replay) {
+        p.targs = p.graph_targs;
+        p.trav_grid = p.graph_trav_grid;
+        p.batch_kind = p.graph_kind;
+        // the fill's shape is not part of the count key
+        p.fill_grid = traverse_grid(p, b.natoms, p.fill_mult, kModeFill, b.fp32, p.batch_kind,
+                                    p.fill_shape, false);
+        NBL_CUDA(cudaGraphLaunch(p.count_graph, st), "count-phase graph");
+        count_launch((int)p.graph_launches);
+    } else {
+        s = enqueue_count(p, b, st);
+        if (s != NBL_SUCCESS) return s;
+    }
     Bufs &B = p.bufs;
     const int64_t N = b.natoms;
     if (sync) {
@@ -743,6 +845,9 @@ nbl_status plan_init(Plan &p, int device_id) {
 void plan_free(Plan &p) {
     DeviceGuard g(p.device);
     if (p.stage_done) cudaEventSynchronize(p.stage_done);
+    drop_count_graph(p);
+    if (p.capture_stream) cudaStreamDestroy(p.capture_stream);
+    p.capture_stream = nullptr;
     p.ws.release();
     if (p.host_small) cudaFreeHost(p.host_small);
     if (p.host_stage) cudaFreeHost(p.host_stage);
@@ -791,6 +896,7 @@ nbl_status nbl_plan_trim(nbl_plan *plan) {
     if (!plan) return set_error(NBL_ERROR_INVALID_ARGUMENT, "null plan");
     DeviceGuard g(plan->p.device);
     cudaDeviceSynchronize();
+    drop_count_graph(plan->p);
     plan->p.ws.release();
     plan->p.have_count = false;
     return NBL_SUCCESS;
@@ -844,7 +950,7 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     cs.warps = cfg->count_warps == 0 ? 4 : cfg->count_warps;
     cs.cand = cfg->count_large_staging;
     cs.group = cfg->count_group == 0 ? 4 : cfg->count_group;
-    fs.warps = cfg->fill_warps == 0 ? 4 : cfg->fill_warps;
+    fs.warps = cfg->fill_warps == 0 ? default_fill_shape().warps : cfg->fill_warps;
     const int itile = cfg->atoms_per_item == 0 ? 32 : cfg->atoms_per_item;
     if (cfg->count_ctas_per_sm < 0 || cfg->count_ctas_per_sm > 64 || cfg->fill_ctas_per_sm < 0 ||
         cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 ||

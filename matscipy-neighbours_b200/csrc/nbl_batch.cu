@@ -55,7 +55,7 @@ __global__ void k_sys_offsets(const int64_t *__restrict__ offsets,
 
 struct TuneChoice {
     int count_mult = 0, count_group = 4, fill_mult = 0, count_tickets = 1, fill_tickets = 1;
-    int count_warps = 4, count_cand = 0, fill_warps = 4, itile = 32;
+    int count_warps = 4, count_cand = 0, fill_warps = 8, itile = 32;
     float count_ms = 0.f, fill_ms = 0.f;
 };
 

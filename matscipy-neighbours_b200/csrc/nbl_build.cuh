@@ -63,6 +63,7 @@ struct TraverseArgs {
     const float *amax;
     const float *pt32;        // per-type squared cutoffs, FP32
     const double *pt64;       // per-type squared cutoffs, FP64
+    int64_t natoms;           // atoms of the batch (offsets[natoms] = pair total)
     int32_t *counts;          // COUNT: per global atom
     const int64_t *offsets;   // FILL: row starts per global atom (+1)
     int32_t *first;
@@ -121,6 +122,13 @@ struct TravShape {
     int cand = 0;
     int group = 4;
 };
+// The fill's default shape: 8-warp CTAs (two per SM with 128 registers a
+// thread, which the fill uses without spilling).
+inline TravShape default_fill_shape() {
+    TravShape s;
+    s.warps = 8;
+    return s;
+}
 
 cudaError_t launch_bin(const BinArgs &a, cudaStream_t st);
 cudaError_t launch_gather(const GatherArgs &a, cudaStream_t st);

@@ -286,6 +286,7 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     ta.i_lo = 0;
     ta.i_hi = INT64_MAX;
     ta.itile = 32;
+    ta.natoms = N;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // two whole waves of each pass's resident CTAs

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -82,6 +83,19 @@ struct Workspace {
 // Full waves of resident CTAs in the default grid of a pair pass.
 constexpr int kAutoWaves = 2;
 
+// Everything that shapes the count phase's launches on a plan: when two
+// consecutive single calls have the same key, the second captures the count
+// phase into a CUDA graph and later ones replay it (compared bytewise; the
+// constructor zeroes the padding).
+struct CountKey {
+    const void *ws_base, *pos, *per_atom, *types;
+    int64_t natoms, table_size, mask_cap, pt_size, i_lo, i_hi;
+    int32_t nsys, grid, key_bits, fp32, kind, itile, nvisit_tab;
+    int32_t count_mult, count_warps, count_cand, count_group, count_tickets;
+    CountKey() { std::memset(this, 0, sizeof(*this)); }
+    bool operator==(const CountKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
 struct Plan {
     int device = 0;
     int num_sms = 148;
@@ -98,7 +112,7 @@ struct Plan {
     int count_mult = 0;
     int fill_mult = 0;
     TravShape count_shape;
-    TravShape fill_shape;
+    TravShape fill_shape = default_fill_shape();
     int itile = 32;
     // Work items by atomic ticket (else a fixed warp stride) in each pass.
     bool count_tickets = true;
@@ -120,7 +134,19 @@ struct Plan {
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_done = nullptr;
     bool stage_in_flight = false;
+    // Count-phase graph of the single-call path (see CountKey).
+    CountKey last_key, graph_key;
+    bool have_last_key = false;
+    bool graphs_off = false;        // capture failed once: direct launches only
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t count_graph = nullptr;
+    long long graph_launches = 0;   // kernels in the graph (launch accounting)
+    TraverseArgs graph_targs{};     // host state the capture left behind
+    int graph_trav_grid = 0, graph_kind = 0;
 };
+
+// Drops the plan's count-phase graph (its pointers refer to the workspace).
+void drop_count_graph(Plan &p);
 
 // An NVTX range over one host-side stage (bin, sort, gather, count, scan,
 // fill): profilers show the stages of a call by name and can filter their

@@ -76,13 +76,40 @@ struct FillTile {
     static constexpr int kCand = FP32 ? 64 : 32;
 };
 
+// One visited segment, read by the fill with three wide loads: its offset
+// vector (FP64, the reference's order), the image shift of the visited cell
+// and bj = (first sorted atom of the cell) - (first candidate index of the
+// segment), so candidate kk of the segment is sorted atom bj + kk.
+struct __align__(16) SegRec {
+    double off[3];
+    int32_t m[3];
+    int32_t bj;
+};
+
 struct SegSmem {
-    double off[kSeg][3];
+    SegRec rec[kSeg];
     float off32[kSeg][3];
-    int32_t m[kSeg][3];
     int32_t b[kSeg];
     int32_t pref[kSeg + 1];
 };
+
+// A segment record's values (offset vector and image shift) in registers.
+struct SegVals {
+    double o0, o1, o2;
+    int32_t m0, m1, m2;
+};
+__device__ __forceinline__ SegVals seg_vals(const SegRec &g) {
+    const double2 o01 = *reinterpret_cast<const double2 *>(&g.off[0]);
+    const int4 o2m = *reinterpret_cast<const int4 *>(&g.off[2]);
+    SegVals v;
+    v.o0 = o01.x;
+    v.o1 = o01.y;
+    v.o2 = __hiloint2double(o2m.y, o2m.x);
+    v.m0 = o2m.z;
+    v.m1 = o2m.w;
+    v.m2 = g.m[2];
+    return v;
+}
 
 template <bool FP32, int CAND>
 struct __align__(16) CountSmem {
@@ -243,9 +270,9 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         sg.b[lane] = sl.x;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            sg.off[lane][k] = offd[k];
+            sg.rec[lane].off[k] = offd[k];
             sg.off32[lane][k] = off32[k];
-            sg.m[lane][k] = m[k];
+            sg.rec[lane].m[k] = m[k];
         }
         zero = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
     }
@@ -256,7 +283,10 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         if (lane >= d) incl += o;
     }
     total = __shfl_sync(full, incl, 31);
-    if (lane < nseg) sg.pref[lane] = incl - len;
+    if (lane < nseg) {
+        sg.pref[lane] = incl - len;
+        sg.rec[lane].bj = sg.b[lane] - (incl - len);
+    }
     if (lane == 0) sg.pref[nseg] = total;
     const unsigned zm = __ballot_sync(full, zero);
     zs = zm ? __ffs(zm) - 1 : -1;
@@ -353,7 +383,7 @@ __device__ __noinline__ bool resolve_exact(const SegSmem &sg, const TraverseArgs
                                            float wi) {
     const int seg = seg_of(sg, nseg, kk);
     const int32_t sj = sg.b[seg] + (kk - sg.pref[seg]);
-    return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], sg.off[seg], wi,
+    return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], sg.rec[seg].off, wi,
                               a.pos32[sj].w);
 }
 
@@ -412,7 +442,7 @@ __device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const Se
             const int seg = seg_of(sg, nseg, kb + k);
             float tj = 0.f;
             if (KIND == kCutPerType) tj = a.pos32[sg.b[seg] + (kb + k - sg.pref[seg])].w;
-            hit = exact_inside<KIND>(H, a, pi64, pj, sg.off[seg], pi32.w, tj);
+            hit = exact_inside<KIND>(H, a, pi64, pj, sg.rec[seg].off, pi32.w, tj);
         }
         return __ballot_sync(full, hit);
     }
@@ -645,6 +675,17 @@ k_count(TraverseArgs a) {
                                         r2g[2 * h] = r2.x;
                                         r2g[2 * h + 1] = r2.y;
                                     }
+                                    if (KIND != kCutScalar) {
+                                        // Pair thresholds never exceed the binning
+                                        // cutoff's: a chunk with no candidate inside it
+                                        // for any atom of the sweep has no hit and no
+                                        // guard-band candidate, so the per-pair
+                                        // thresholds are skipped (its words stay 0).
+                                        float r2min = r2g[0];
+#pragma unroll
+                                        for (int g = 1; g < GROUP; g++) r2min = fminf(r2min, r2g[g]);
+                                        if (!__any_sync(full, r2min < H.hi_rc)) continue;
+                                    }
 #pragma unroll
                                     for (int g = 0; g < GROUP; g++) {
                                         const float r2 = r2g[g];
@@ -773,7 +814,7 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
         w.il = a0 + al;
         w.slot = sm.abase[al] + P;
         w.seg = seg_of_tab(sm, nseg, kk);
-        const int32_t sj = sm.sg.b[w.seg] + (kk - sm.sg.pref[w.seg]);
+        const int32_t sj = sm.sg.rec[w.seg].bj + kk;
         w.pj = a.pos64[sj];
         w.aj = a.aux[sj];
     }
@@ -782,16 +823,18 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
 
 // Compute and store one pair (exact FP64 D and d, S, i, j).  ALL5: all five
 // outputs requested and no neighbour matrix (no per-pair output checks).
+// check: test the slot against the output capacity (warp-uniform; false when
+// the whole list is known to fit).
 template <bool FP32, bool ALL5>
 __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const TraverseArgs &a,
-                                           const Hot &H, const PairWork &w) {
+                                           const Hot &H, const PairWork &w, bool check) {
     if (!w.act) return;
     const double4 pi = sm.i64[w.il];
     const int4 ai = sm.iaux[w.il];
-    const int seg = w.seg;
-    const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
-    const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
-    const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
+    const SegVals g = seg_vals(sm.sg.rec[w.seg]);
+    const double dx = dadd(dsub(w.pj.x, pi.x), g.o0);
+    const double dy = dadd(dsub(w.pj.y, pi.y), g.o1);
+    const double dz = dadd(dsub(w.pj.z, pi.z), g.o2);
     const int32_t jl = (int32_t)(w.aj.x - H.atom_base);
     if (!ALL5 && a.mat_k > 0) {
         const long long rank = w.slot - (long long)a.offsets[ai.x];
@@ -805,7 +848,7 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
         return;
     }
     const long long slot = w.slot;
-    if (slot >= a.capacity) {
+    if (check && slot >= a.capacity) {
         atomicOr(a.err, kErrCapacity);
         return;
     }
@@ -823,9 +866,9 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
     }
     if (ALL5 || a.shift) {
         int32_t *Sv = a.shift + 3 * slot;
-        __stcs(Sv, ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + sm.sg.m[seg][0]);
-        __stcs(Sv + 1, ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + sm.sg.m[seg][1]);
-        __stcs(Sv + 2, ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + sm.sg.m[seg][2]);
+        __stcs(Sv, ai.y - ((H.pbc_bits & 1) ? w.aj.y : 0) + g.m0);
+        __stcs(Sv + 1, ai.z - ((H.pbc_bits & 2) ? w.aj.z : 0) + g.m1);
+        __stcs(Sv + 2, ai.w - ((H.pbc_bits & 4) ? w.aj.w : 0) + g.m2);
     }
 }
 
@@ -846,9 +889,10 @@ __device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc
     if (w.act) {
         const double4 pi = sm.i64[w.il];
         const int seg = w.seg;
-        const double dx = dadd(dsub(w.pj.x, pi.x), sm.sg.off[seg][0]);
-        const double dy = dadd(dsub(w.pj.y, pi.y), sm.sg.off[seg][1]);
-        const double dz = dadd(dsub(w.pj.z, pi.z), sm.sg.off[seg][2]);
+        const SegVals g = seg_vals(sm.sg.rec[seg]);
+        const double dx = dadd(dsub(w.pj.x, pi.x), g.o0);
+        const double dy = dadd(dsub(w.pj.y, pi.y), g.o1);
+        const double dz = dadd(dsub(w.pj.z, pi.z), g.o2);
         const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
         const double ir2 = 1.0 / r2;
         const double s2 = a.lj_sig2 * ir2;
@@ -901,6 +945,8 @@ k_fill(TraverseArgs a) {
     const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
     const bool all_rows = all_rows_of(a);
+    // every slot of the list is below the output capacity: no per-pair test
+    const bool cap_ok = a.offsets[a.natoms] <= a.capacity;
     ItemLoop L(a, gwarp, nitems, lane, true);
     while (L.it < nitems) {
         L.prefetch(a, nwarps, nitems, lane, true);
@@ -1082,7 +1128,7 @@ k_fill(TraverseArgs a) {
                             if (LJ)
                                 lj_round<FP32>(sm, facc, a, cur, lane);
                             else
-                                store_pair<FP32, ALL5>(sm, a, H, cur);
+                                store_pair<FP32, ALL5>(sm, a, H, cur, !cap_ok);
                             cur = nxt;
                         }
                         __syncwarp();

@@ -424,7 +424,8 @@ def run_device(quantities, origin, cell, inv, pbc8, pos_t, host_pos, rc, per_ato
     req = make_request(flags, origin, cell, inv, pbc8, nat, ptr, on_dev, rc, per_atom,
                        per_type_sq, ncut, types, device_id)
     npairs = ctypes.c_int64()
-    with torch.cuda.device(dev):
+    ctx = torch.cuda.device(dev) if torch.cuda.current_device() != device_id else _NO_CONTEXT
+    with ctx:
         if atom_range is not None:
             check(lib.nbl_set_atom_range(plan, int(atom_range[0]), int(atom_range[1])))
         try:
@@ -436,14 +437,41 @@ def run_device(quantities, origin, cell, inv, pbc8, pos_t, host_pos, rc, per_ato
                 # later calls on this thread's plan build full lists again.
                 lib.nbl_set_atom_range(plan, 0, -1)
         n = int(npairs.value)
-        tdt = {np.int32: torch.int32, np.float64: torch.float64}
-        bufs = {}
-        for ch in set(quantities):
-            extra, dt = _SHAPES[ch]
-            bufs[ch] = torch.empty((n,) + extra, dtype=tdt[dt], device=dev)
+        bufs = _device_outputs(torch, quantities, n, dev)
         if n:
             o = _outputs_struct(bufs, lambda t: t.data_ptr())
             check(lib.nbl_fill(plan, ctypes.byref(o), ctypes.c_void_p(stream.cuda_stream)))
+    return bufs
+
+
+class _NoContext:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+_NO_CONTEXT = _NoContext()
+
+
+def _device_outputs(torch, quantities, n, dev):
+    """The requested outputs as views of one device allocation (each starting
+    on a 256-byte boundary): one allocator call instead of one per quantity.
+    The views keep the allocation alive together."""
+    chars = [ch for ch in "ijDdS" if ch in quantities]
+    offs, total = {}, 0
+    for ch in chars:
+        extra, dt = _SHAPES[ch]
+        offs[ch] = total
+        total += (n * (3 if extra else 1) * np.dtype(dt).itemsize + 255) & ~255
+    raw = torch.empty(max(total, 1), dtype=torch.uint8, device=dev)
+    bufs = {}
+    for ch in chars:
+        extra, dt = _SHAPES[ch]
+        tdt = torch.int32 if dt == np.int32 else torch.float64
+        nbytes = n * (3 if extra else 1) * np.dtype(dt).itemsize
+        bufs[ch] = raw[offs[ch]:offs[ch] + nbytes].view(tdt).view((n,) + extra)
     return bufs
 
 
