@@ -353,6 +353,35 @@ __device__ __forceinline__ void stage_segs(CandT<FP32> *cand, const SegSmem &sg,
     __syncwarp();
 }
 
+// FP32 staging for the count, as stage_segs but without a dependent global
+// load per candidate: with short cell runs each lane (segment) starts
+// asynchronous copies of its whole run, waits for them, and adds its
+// segment's offset to the run in shared memory.
+__device__ __forceinline__ void stage_segs_async(float4 *cand, const SegSmem &sg,
+                                                 const TraverseArgs &a, int nseg, int kb, int nk,
+                                                 int nkp, int lane) {
+    if (sg.pref[nseg] > 48 * nseg) {
+        stage_segs<true>(cand, sg, a, nseg, kb, nk, nkp, lane);
+        return;
+    }
+    __syncwarp();
+    if (lane < nseg) {
+        const int s0 = max(sg.pref[lane], kb), s1 = min(sg.pref[lane + 1], kb + nk);
+        const int jb = sg.b[lane] - sg.pref[lane];
+        for (int kk = s0; kk < s1; kk++) cp_async16(&cand[kk - kb], &a.pos32[jb + kk]);
+        cp_async_wait();
+        const float ox = sg.off32[lane][0], oy = sg.off32[lane][1], oz = sg.off32[lane][2];
+#pragma unroll 4
+        for (int kk = s0; kk < s1; kk++) {
+            const float4 p = cand[kk - kb];
+            cand[kk - kb] = make_float4(p.x + ox, p.y + oy, p.z + oz, p.w);
+        }
+    }
+    for (int k = nk + lane; k < nkp; k += 32)
+        cand[k] = make_float4(kFarCand, kFarCand, kFarCand, 0.f);
+    __syncwarp();
+}
+
 // The reference's exact FP64 inclusion test (neighbour_visit.hh:88-109).
 template <int KIND>
 __device__ __forceinline__ bool exact_inside(const Hot &H, const TraverseArgs &a,
@@ -622,7 +651,10 @@ k_count(TraverseArgs a) {
                     const int nk = min(kCand, total - kb);
                     const int nkp = (nk + 31) & ~31;
                     const int nck = nkp >> 5;
-                    stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
+                    if constexpr (FP32)
+                        stage_segs_async(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
+                    else
+                        stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kb, nk, nkp, lane);
                     if constexpr (FP32) {
                         // GROUP atoms per pass over the tile
                         for (int g0 = 0; g0 < ni; g0 += GROUP) {
@@ -691,9 +723,8 @@ k_count(TraverseArgs a) {
                                         const float r2 = r2g[g];
                                         float lo, hi;
                                         thresholds<KIND>(H, a, pg[g].w, cv.w, lo, hi);
-                                        const bool notself = k != ks[g];
-                                        m[g] = __ballot_sync(full, (r2 < lo) && notself);
-                                        amb[g] = !(r2 < lo) && (r2 < hi) && notself;
+                                        m[g] = __ballot_sync(full, r2 < lo);
+                                        amb[g] = !(r2 < lo) && (r2 < hi);
                                         amb_any |= amb[g];
                                     }
                                     if (__any_sync(full, amb_any)) {
@@ -710,6 +741,14 @@ k_count(TraverseArgs a) {
                                     const bool mine = lane == ch - cb;
 #pragma unroll
                                     for (int g = 0; g < GROUP; g++) mw[g] = mine ? m[g] : mw[g];
+                                }
+                                // An atom is never its own neighbour: its candidate at the
+                                // zero offset (staged position ks) is cleared once per block
+                                // instead of being tested in every chunk.
+#pragma unroll
+                                for (int g = 0; g < GROUP; g++) {
+                                    if (ks[g] >= 0 && lane == (ks[g] >> 5) - cb)
+                                        mw[g] &= ~(1u << (ks[g] & 31));
                                 }
 #pragma unroll
                                 for (int g = 0; g < GROUP; g++)
