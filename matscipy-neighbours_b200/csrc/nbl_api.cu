@@ -1248,6 +1248,8 @@ int nbl_has_gpu(void) {
 
 int nbl_device_type(void) { return 2; }
 
-const char *nbl_version(void) { return "nbl_b200 0.1.0 (sm_100a)"; }
+const char *nbl_version(void) {
+    return kChecked ? "nbl_b200 0.1.0 (sm_100a, checked)" : "nbl_b200 0.1.0 (sm_100a)";
+}
 
 }  // extern "C"

@@ -40,6 +40,28 @@ constexpr int kErrRange = 1;      // non-finite or out-of-range position
 constexpr int kErrCapacity = 2;   // output slot beyond capacity
 constexpr int kErrInternal = 4;   // a device-side bound was hit
 
+// Checked build (-DNBL_CHECKED=1, libnbl_b200_checked.so): the traversal
+// kernels also test the indices that the release build holds in bounds by
+// construction -- every cell slice within [0, natoms], every candidate and
+// home atom below natoms, every hit word below the pool size, and every
+// output slot inside its own row [offsets[i], offsets[i+1]).  A failed test
+// sets kErrInternal and skips the access; it never traps.
+#ifndef NBL_CHECKED
+#define NBL_CHECKED 0
+#endif
+constexpr bool kChecked = NBL_CHECKED != 0;
+
+// True (and kErrInternal recorded) when a checked build sees `bad`.
+__device__ __forceinline__ bool checked_fail(bool bad, int *err) {
+    if constexpr (kChecked) {
+        if (bad) {
+            atomicOr(err, kErrInternal);
+            return true;
+        }
+    }
+    return false;
+}
+
 // Composite key layout of the hashed grid: system id above bit 43.
 constexpr int kHashSysShift = 43;
 constexpr unsigned long long kHashEmpty = ~0ull;

@@ -266,6 +266,8 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         }
         int2 sl = make_int2(0, 0);
         if (ok) sl = cell_lookup(a, S, c.sys, cj[0], cj[1], cj[2]);
+        if (checked_fail(sl.x < 0 || sl.y < sl.x || (long long)sl.y > a.natoms, a.err))
+            sl = make_int2(0, 0);
         len = sl.y - sl.x;
         sg.b[lane] = sl.x;
 #pragma unroll
@@ -536,6 +538,18 @@ __device__ __forceinline__ bool all_rows_of(const TraverseArgs &a) {
     return a.i_lo <= 0 && a.i_hi >= (1ll << 40);
 }
 
+// Checked build: the work item's tile lies inside the sorted atoms.
+__device__ __forceinline__ bool item_bad(const TraverseArgs &a, const WorkItem &w) {
+    return checked_fail(w.ib < 0 || w.nt < 0 || w.nt > kITile ||
+                            (long long)w.ib + w.nt > a.natoms,
+                        a.err);
+}
+
+// Checked build: hit word `idx` lies inside the pool.
+__device__ __forceinline__ bool word_bad(const TraverseArgs &a, long long idx) {
+    return checked_fail(idx < 0 || idx >= a.mask_cap, a.err);
+}
+
 // Position of the (r+1)-th set bit of w (r < popc(w)).
 __device__ __forceinline__ int nth_set_bit(unsigned w, int r) {
     int pos = 0;
@@ -588,6 +602,7 @@ k_count(TraverseArgs a) {
 
         do {
             const int ib = L.rec.ib;
+            if (item_bad(a, L.rec)) break;
             // The tile's atoms whose original index lies in [i_lo, i_hi),
             // compacted in order (all of them unless the rows are split); with
             // all rows they are copied asynchronously and land during the
@@ -757,7 +772,8 @@ k_count(TraverseArgs a) {
                                     const long long w0 = mbase + (kb >> 5) + cb + lane;
 #pragma unroll
                                     for (int g = 0; g < GROUP; g++) {
-                                        if (g0 + g < ni)
+                                        if (g0 + g < ni &&
+                                            !word_bad(a, w0 + (long long)(g0 + g) * nchunks_all))
                                             a.mask_pool[w0 + (long long)(g0 + g) * nchunks_all] =
                                                 mw[g];
                                     }
@@ -787,9 +803,10 @@ k_count(TraverseArgs a) {
                                 cnt += __popc(mask);
                                 mword = (lane == (ch & 31)) ? mask : mword;
                                 if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
-                                    if (lane <= (ch & 31))
-                                        a.mask_pool[mbase + (long long)il * nchunks_all +
-                                                    (kb >> 5) + (ch & ~31) + lane] = mword;
+                                    const long long wi = mbase + (long long)il * nchunks_all +
+                                                         (kb >> 5) + (ch & ~31) + lane;
+                                    if (lane <= (ch & 31) && !word_bad(a, wi))
+                                        a.mask_pool[wi] = mword;
                                 }
                             }
                             if (lane == 0) sm.icount[il] += cnt;
@@ -798,7 +815,9 @@ k_count(TraverseArgs a) {
                     }
                 }
             }
-            if (lane < ni) a.counts[sm.iatom[lane]] = sm.icount[lane];
+            if (lane < ni &&
+                !checked_fail(sm.iatom[lane] < 0 || sm.iatom[lane] >= a.natoms, a.err))
+                a.counts[sm.iatom[lane]] = sm.icount[lane];
             __syncwarp();
         } while (0);
         L.step();
@@ -854,6 +873,10 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
         w.slot = sm.abase[al] + P;
         w.seg = seg_of_tab(sm, nseg, kk);
         const int32_t sj = sm.sg.rec[w.seg].bj + kk;
+        if (checked_fail(sj < 0 || sj >= a.natoms, a.err)) {
+            w.act = false;
+            return w;
+        }
         w.pj = a.pos64[sj];
         w.aj = a.aux[sj];
     }
@@ -870,6 +893,13 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
     if (!w.act) return;
     const double4 pi = sm.i64[w.il];
     const int4 ai = sm.iaux[w.il];
+    if constexpr (kChecked) {  // the slot lies in its own row
+        if (checked_fail(ai.x < 0 || ai.x >= a.natoms, a.err)) return;
+        if (checked_fail(w.slot < (long long)a.offsets[ai.x] ||
+                             w.slot >= (long long)a.offsets[ai.x + 1],
+                         a.err))
+            return;
+    }
     const SegVals g = seg_vals(sm.sg.rec[w.seg]);
     const double dx = dadd(dsub(w.pj.x, pi.x), g.o0);
     const double dy = dadd(dsub(w.pj.y, pi.y), g.o1);
@@ -995,6 +1025,7 @@ k_fill(TraverseArgs a) {
 
         do {
             const int ib = L.rec.ib;
+            if (item_bad(a, L.rec)) break;
             int ni;
             // The tile's atoms: with all rows copied asynchronously (they land
             // during the segment set-up; the row starts follow once their
@@ -1029,7 +1060,9 @@ k_fill(TraverseArgs a) {
                     sm.i64[c2] = a.pos64[si];
                     sm.iaux[c2] = ax;
                     sm.isi[c2] = si;
-                    sm.icur[c2] = (long long)a.offsets[ax.x];
+                    sm.icur[c2] = checked_fail(ax.x >= a.natoms, a.err)
+                                      ? 0ll
+                                      : (long long)a.offsets[ax.x];
                     if (LJ) facc[c2][0] = facc[c2][1] = facc[c2][2] = facc[c2][3] = 0.0;
                 }
                 __syncwarp();
@@ -1042,14 +1075,20 @@ k_fill(TraverseArgs a) {
             const bool words0 =
                 mb0 >= 0 && c.nvisit <= kSeg && ni * nch0 <= kWinWords && nch0 * 32 <= kRange;
             if (words0)
-                for (int w = lane; w < ni * nch0; w += 32) cp_async4(&sm.mw[w], &a.mask_pool[mb0 + w]);
+                for (int w = lane; w < ni * nch0; w += 32)
+                    if (!word_bad(a, mb0 + w)) cp_async4(&sm.mw[w], &a.mask_pool[mb0 + w]);
             for (int vb = 0; vb < c.nvisit; vb += kSeg) {
                 int nseg, total, zs;
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 if (vb == 0) {
                     cp_async_wait();
                     __syncwarp();
-                    if (off_pending && lane < ni) my_off = (long long)a.offsets[sm.iaux[lane].x];
+                    if (off_pending && lane < ni) {
+                        const int ax = sm.iaux[lane].x;
+                        my_off = checked_fail(ax < 0 || ax >= a.natoms, a.err)
+                                     ? 0ll
+                                     : (long long)a.offsets[ax];
+                    }
                 }
                 const int nchunks = (total + 31) >> 5;
                 const long long mbase =
@@ -1080,8 +1119,9 @@ k_fill(TraverseArgs a) {
                         } else if (mbase >= 0) {
                             for (int w = lane; w < nw; w += 32) {
                                 const int al = div_small(w, nch, inv_nch);
-                                sm.mw[w] = a.mask_pool[mbase + (long long)(a0 + al) * nchunks +
-                                                       (kr >> 5) + (w - al * nch)];
+                                const long long wi = mbase + (long long)(a0 + al) * nchunks +
+                                                     (kr >> 5) + (w - al * nch);
+                                sm.mw[w] = word_bad(a, wi) ? 0u : a.mask_pool[wi];
                             }
                         } else {
                             for (int kt = 0; kt < nrange; kt += kCand) {
@@ -1183,7 +1223,8 @@ k_fill(TraverseArgs a) {
                 __syncwarp();
             }
             // --- fill must land exactly on the next row; matrix row lengths --------
-            if (lane < ni) {
+            if (lane < ni && !checked_fail(sm.iaux[lane].x < 0 ||
+                                               sm.iaux[lane].x >= a.natoms, a.err)) {
                 const int ax = sm.iaux[lane].x;
                 const long long end = (long long)a.offsets[ax + 1];
                 if (sm.icur[lane] != end) atomicOr(a.err, kErrInternal);

@@ -16,12 +16,18 @@ buffers, streams and DLPack interop.
 """
 
 import ctypes
+import os
 import pathlib
 import threading
 
 import numpy as np
 
-_LIB_PATH = pathlib.Path(__file__).resolve().with_name("libnbl_b200.so")
+# MATSCIPY_NEIGHBOURS_CHECKED=1 selects the checked build of the engine (the
+# same kernels with every device-side index tested; built by
+# ``build.py --checked``).
+CHECKED = os.environ.get("MATSCIPY_NEIGHBOURS_CHECKED", "0") not in ("", "0")
+_LIB_PATH = pathlib.Path(__file__).resolve().with_name(
+    "libnbl_b200_checked.so" if CHECKED else "libnbl_b200.so")
 
 QUANTITY_FIRST = 1
 QUANTITY_SECOND = 2
@@ -85,7 +91,8 @@ def _load():
     if not _LIB_PATH.exists():
         raise ImportError(
             f"{_LIB_PATH.name} is not built; run "
-            "`python matscipy-neighbours_b200/build.py` (needs nvcc)")
+            "`python matscipy-neighbours_b200/build.py"
+            f"{' --checked' if CHECKED else ''}` (needs nvcc)")
     lib = ctypes.CDLL(str(_LIB_PATH))
     P = ctypes.c_void_p
     sigs = {

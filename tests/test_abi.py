@@ -29,6 +29,21 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_checked_build_exports_the_same_entry_points():
+    """The checked build (build.py --checked) is a drop-in for the release
+    library: same symbols, its version string says which it is."""
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    path = ext._LIB_PATH.with_name("libnbl_b200_checked.so")
+    if not path.exists():
+        pytest.skip("checked build not built")
+    lib = ctypes.CDLL(str(path))
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    lib.nbl_version.restype = ctypes.c_char_p
+    assert b"checked" in lib.nbl_version()
+    assert b"checked" not in ext.lib.nbl_version()
+
+
 def test_library_is_sm100a_build():
     from matscipy_neighbours import _matscipy_neighbours as ext
     assert b"sm_100a" in ext.lib.nbl_version()
