@@ -168,6 +168,13 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
                                           1 = 768 / 384
      atoms_per_item                       cell-occupancy tile: atoms of one
                                           cell per work item, 1..32 (32)
+     cells_per_item                       home cells one work item may join
+                                          along x when their atoms fit one
+                                          tile: 0 = chosen on the device from
+                                          the mean cell occupancy (sparse
+                                          grids join up to 8), 1 = one cell
+                                          per item, 2..8 = at most that many
+                                          (dense grid and FP32 filter only)
    No reference counterpart (the reference has no tuner). */
 typedef struct nbl_launch_config {
     int count_ctas_per_sm;
@@ -179,6 +186,7 @@ typedef struct nbl_launch_config {
     int count_group;
     int count_large_staging;
     int atoms_per_item;
+    int cells_per_item;
 } nbl_launch_config;
 
 NBL_API nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *cfg);

@@ -387,9 +387,23 @@ nbl_status finish_batch(Batch &b, int grid_req) {
 static int traverse_grid(const Plan &p, int64_t natoms, int mult, int mode, bool fp32,
                          int kind, const TravShape &shape, bool lj) {
     if (mult <= 0)
-        mult = kAutoWaves * std::max(1, traverse_blocks_per_sm(mode, fp32, kind, shape, lj));
+        mult = kAutoWaves * std::max(1, traverse_blocks_per_sm(mode, fp32, kind, shape, lj,
+                                                               p.targs.runs != 0));
     const int64_t items = std::max<int64_t>((natoms + 3) / 4, 1);
     return (int)std::min<int64_t>((int64_t)p.num_sms * mult, items);
+}
+
+// Home cells per work item the tile builder may join: runs need the dense
+// grid (a run's atoms are contiguous in sorted order), the FP32 filter (the
+// plain FP64 sweep reads each segment's own offset) and the systems' visit
+// tables (a pair's offset vector is looked up there).
+static int run_limit(const Plan &p, const Batch &b) {
+    if (b.grid != kGridDense || !b.fp32 || p.bufs.visit == nullptr) return 1;
+    // left to the device only where the grid is sparse on average (below two
+    // atoms per cell); denser grids keep one cell per item and the kernels
+    // without run handling
+    if (p.max_run == 0 && (double)b.natoms >= 2.0 * (double)b.table_size) return 1;
+    return p.max_run;
 }
 
 // Size the workspace for a batch and copy its inputs and host tables in.
@@ -521,8 +535,8 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     {
         StageRange r("nbl.gather");
         NBL_CUDA(launch_gather(ga, st), "k_gather");
-        NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.items, B.small + 3, N, p.num_sms,
-                              p.itile, st),
+        NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.sys, B.items, B.small + 3, N,
+                              p.num_sms, p.itile, run_limit(p, b), st),
                  "k_tiles");
     }
 
@@ -556,6 +570,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.i_hi = p.i_hi;
     ta.itile = p.itile;
     ta.natoms = N;
+    ta.runs = run_limit(p, b) != 1 ? 1 : 0;
     if (p.i_lo > 0 || p.i_hi < N)
         NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
@@ -602,6 +617,7 @@ static CountKey count_key(const Plan &p, const Batch &b) {
     k.fp32 = b.fp32 ? 1 : 0;
     k.kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
     k.itile = p.itile;
+    k.max_run = run_limit(p, b);
     k.nvisit_tab = p.bufs.visit != nullptr ? 1 : 0;
     k.count_mult = p.count_mult;
     k.count_warps = p.count_shape.warps;
@@ -754,6 +770,7 @@ void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
     cfg->count_group = p.count_shape.group;
     cfg->count_large_staging = p.count_shape.cand;
     cfg->atoms_per_item = p.itile;
+    cfg->cells_per_item = p.max_run;
 }
 
 // Request -> one-system batch.
@@ -953,11 +970,13 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     fs.warps = cfg->fill_warps == 0 ? default_fill_shape().warps : cfg->fill_warps;
     const int itile = cfg->atoms_per_item == 0 ? 32 : cfg->atoms_per_item;
     if (cfg->count_ctas_per_sm < 0 || cfg->count_ctas_per_sm > 64 || cfg->fill_ctas_per_sm < 0 ||
-        cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 ||
-        !traverse_shape_ok(kModeCount, true, cs) || !traverse_shape_ok(kModeFill, true, fs))
+        cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 || cfg->cells_per_item < 0 ||
+        cfg->cells_per_item > kMaxRun || !traverse_shape_ok(kModeCount, true, cs) ||
+        !traverse_shape_ok(kModeFill, true, fs))
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "launch config: CTAs per SM in [0, 64], warps 2, 4 or 8, count group "
-                         "2 or 4, large candidate staging 0 or 1, atoms per item in [1, 32]");
+                         "2 or 4, large candidate staging 0 or 1, atoms per item in [1, 32], "
+                         "cells per item in [0, %d]", kMaxRun);
     plan->p.count_mult = cfg->count_ctas_per_sm;
     plan->p.fill_mult = cfg->fill_ctas_per_sm;
     plan->p.count_tickets = cfg->count_strided == 0;
@@ -965,6 +984,7 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     plan->p.count_shape = cs;
     plan->p.fill_shape = fs;
     plan->p.itile = itile;
+    plan->p.max_run = cfg->cells_per_item;
     return NBL_SUCCESS;
 }
 

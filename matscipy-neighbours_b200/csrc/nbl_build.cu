@@ -210,17 +210,32 @@ k_gather(GatherArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_tiles: work items = (occupied cell, i-tile of `itile` <= 32 atoms)
+// k_tiles: work items = (occupied cell, i-tile of `itile` <= 32 atoms), or
+// runs of consecutive occupied cells along x
 // ---------------------------------------------------------------------------
 // Splitting large cells keeps one warp from holding a whole big cell (a
 // small periodic system often is one cell) while the rest of the GPU idles.
+// Sparse grids (few atoms per cell) instead pack the occupied cells of each
+// aligned block of `R` cells along x into one item when their atoms fit one
+// tile: the run's neighbour cells are then visited once for up to R home
+// cells.  R = max_run, or (max_run == 0) chosen from the mean occupancy:
+// 1 (no runs) at 6 or more atoms per occupied cell, else about itile / (2 x
+// occupancy), at most kMaxRun.  Runs need the dense grid (the run's atoms are
+// contiguous in sorted order) and a +-1 cell scan in every direction.
 __global__ void __launch_bounds__(256)
 k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
-        const int2 *__restrict__ table, WorkItem *__restrict__ items, int *__restrict__ n_items,
-        int itile) {
+        const int2 *__restrict__ table, const SysDev *__restrict__ sys,
+        WorkItem *__restrict__ items, int *__restrict__ n_items, int64_t natoms, int itile,
+        int max_run) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int nh = *n_home;
+    int R = max_run;
+    if (R == 0) {
+        const float occ = (float)natoms / (float)max(nh, 1);
+        R = occ >= 6.f ? 1 : min(kMaxRun, max(1, (int)((float)itile / (2.f * occ))));
+    }
+    R = min(R, kMaxRun);
     for (int base = blockIdx.x * blockDim.x; base < nh; base += gridDim.x * blockDim.x) {
         const int h = base + threadIdx.x;
         int2 hs = make_int2(0, 0);
@@ -229,7 +244,30 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
             hc = home[h];
             hs = table[hc.tidx];
         }
-        const int nt = (hs.y - hs.x + itile - 1) / itile;
+        int nt = (hs.y - hs.x + itile - 1) / itile;
+        int run = 1, run_atoms = 0;
+        if (R > 1 && h < nh) {
+            const SysDev &S = sys[hc.sys];
+            if (S.nscan[0] == 1 && S.nscan[1] == 1 && S.nscan[2] == 1) {
+                const int x = hc.c[0];
+                const int xb = (x / R) * R, xe = min(xb + R, S.n[0]);
+                int total = 0, first = -1, last = -1;
+                for (int xc = xb; xc < xe; xc++) {
+                    const int2 sl = table[hc.tidx + (xc - x)];
+                    const int n = sl.y - sl.x;
+                    if (n > 0) {
+                        total += n;
+                        if (first < 0) first = xc;
+                        last = xc;
+                    }
+                }
+                if (total <= itile && first != last) {  // two or more occupied cells
+                    nt = (x == first) ? 1 : 0;
+                    run = last - first + 1;
+                    run_atoms = total;
+                }
+            }
+        }
         int incl = nt;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -247,21 +285,22 @@ k_tiles(const HomeCell *__restrict__ home, const int *__restrict__ n_home,
             w.c[2] = hc.c[2];
             w.sys = hc.sys;
             w.ib = hs.x + itile * t;
-            w.nt = min(itile, hs.y - w.ib);
+            w.nt = run > 1 ? run_atoms : min(itile, hs.y - w.ib);
             w.tidx = hc.tidx;
-            w.pad = 0;
+            w.run = run;
             items[first + t] = w;
         }
     }
 }
 
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         WorkItem *items, int *n_items, int64_t natoms, int num_sms, int itile,
-                         cudaStream_t st) {
+                         const SysDev *sys, WorkItem *items, int *n_items, int64_t natoms,
+                         int num_sms, int itile, int max_run, cudaStream_t st) {
     if (natoms <= 0) return cudaSuccess;
-    if (itile < 1 || itile > 32) return cudaErrorInvalidValue;
+    if (itile < 1 || itile > 32 || max_run < 0) return cudaErrorInvalidValue;
     const int64_t blocks = std::min<int64_t>((natoms + 255) / 256, (int64_t)num_sms * 4);
-    k_tiles<<<(unsigned)blocks, 256, 0, st>>>(home, n_home, table, items, n_items, itile);
+    k_tiles<<<(unsigned)blocks, 256, 0, st>>>(home, n_home, table, sys, items, n_items, natoms,
+                                              itile, max_run);
     count_launch();
     return cudaGetLastError();
 }
@@ -407,10 +446,11 @@ bool traverse_shape_ok(int mode, bool fp32, const TravShape &s) {
     return (s.cand == 0 || s.cand == 1) && (!fp32 || s.group == 2 || s.group == 4);
 }
 
-int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape, bool lj) {
-    // cached per device, pass, precision, kind and shape
+int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape, bool lj,
+                           bool runs) {
+    // cached per device, pass, precision, kind, shape and run instantiation
     constexpr int kDev = 16;
-    static std::atomic<int> cache[kDev][2][2][3][3][2][2][2];
+    static std::atomic<int> cache[kDev][2][2][3][3][2][2][2][2];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDev) {
         cudaGetLastError();
@@ -421,17 +461,23 @@ int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape
     const int wi = shape.warps == 2 ? 0 : (shape.warps == 8 ? 2 : 1);
     const int ci = shape.cand != 0 ? 1 : 0;
     const int gi = shape.group == 2 ? 0 : 1;
+    runs = runs && fp32;  // runs are only built for the FP32 filter
+    const int ri = runs ? 1 : 0;
     if (dev >= 0) {
-        const int c = cache[dev][mi][fi][ki][wi][ci][gi][li].load(std::memory_order_relaxed);
+        const int c = cache[dev][mi][fi][ki][wi][ci][gi][li][ri].load(std::memory_order_relaxed);
         if (c > 0) return c;
     }
     int n = 0;
     if (mode == kModeCount)
-        n = fp32 ? occupancy_count_fp32(kind, shape) : occupancy_count_fp64(kind, shape);
+        n = !fp32 ? occupancy_count_fp64(kind, shape)
+                  : (runs ? occupancy_count_fp32_runs(kind, shape)
+                          : occupancy_count_fp32(kind, shape));
     else
-        n = fp32 ? occupancy_fill_fp32(kind, shape, lj) : occupancy_fill_fp64(kind, shape, lj);
+        n = !fp32 ? occupancy_fill_fp64(kind, shape, lj)
+                  : (runs ? occupancy_fill_fp32_runs(kind, shape, lj)
+                          : occupancy_fill_fp32(kind, shape, lj));
     if (dev >= 0 && n > 0)
-        cache[dev][mi][fi][ki][wi][ci][gi][li].store(n, std::memory_order_relaxed);
+        cache[dev][mi][fi][ki][wi][ci][gi][li][ri].store(n, std::memory_order_relaxed);
     return n;
 }
 
@@ -439,11 +485,15 @@ cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a
                             int grid, cudaStream_t st, const TravShape &shape) {
     if (grid <= 0) return cudaSuccess;
     if (!traverse_shape_ok(mode, fp32, shape)) return cudaErrorInvalidValue;
-    if (mode == kModeCount)
-        return fp32 ? launch_count_fp32(kind, a, grid, st, shape)
-                    : launch_count_fp64(kind, a, grid, st, shape);
-    return fp32 ? launch_fill_fp32(kind, a, grid, st, shape)
-                : launch_fill_fp64(kind, a, grid, st, shape);
+    if (!fp32) {
+        return mode == kModeCount ? launch_count_fp64(kind, a, grid, st, shape)
+                                  : launch_fill_fp64(kind, a, grid, st, shape);
+    }
+    if (a.runs)  // the items may be runs of several home cells
+        return mode == kModeCount ? launch_count_fp32_runs(kind, a, grid, st, shape)
+                                  : launch_fill_fp32_runs(kind, a, grid, st, shape);
+    return mode == kModeCount ? launch_count_fp32(kind, a, grid, st, shape)
+                              : launch_fill_fp32(kind, a, grid, st, shape);
 }
 
 }  // namespace nbl

@@ -111,6 +111,9 @@ struct TraverseArgs {
     // Nonzero: *item_next is already zero (the count phase's init kernel
     // cleared it), so the launch skips its reset.
     int ticket_ready;
+    // Nonzero: k_tiles may have joined home cells into runs (WorkItem::run),
+    // so the pair passes use the instantiations that take them.
+    int runs;
 };
 
 // Launch shape of one pair pass: warps per CTA (2, 4 or 8, i.e. 64, 128 or
@@ -152,17 +155,20 @@ cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStrea
 cudaError_t launch_init(const SysDev *sys, int nsys, VisitDev *visit, int *small, int2 *table,
                         int64_t ntable, float *amax, unsigned long long *hkey, int num_sms,
                         cudaStream_t st);
-// Work items: each occupied cell cut into tiles of `itile` (<= 32) atoms.
+// Work items: each occupied cell cut into tiles of `itile` (<= 32) atoms, or
+// runs of up to `max_run` occupied cells along x (0: chosen from the mean
+// occupancy; 1: no runs; runs need the dense grid and are only taken where
+// every direction scans one cell each way).
 cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *table,
-                         WorkItem *items, int *n_items, int64_t natoms, int num_sms, int itile,
-                         cudaStream_t st);
+                         const SysDev *sys, WorkItem *items, int *n_items, int64_t natoms,
+                         int num_sms, int itile, int max_run, cudaStream_t st);
 cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a,
                             int grid, cudaStream_t st, const TravShape &shape = TravShape());
 // CTAs of the pair pass (mode, precision, cutoff kind, shape, force sink)
 // resident per SM on the current device: the grid of one full wave is this
 // times the SM count.  0 on error.
 int traverse_blocks_per_sm(int mode, bool fp32, int kind, const TravShape &shape = TravShape(),
-                           bool lj = false);
+                           bool lj = false, bool runs = false);
 // Candidates one count warp stages per sweep for a shape.
 constexpr int count_candidates(bool fp32, int cand) {
     return (fp32 ? 384 : 192) * (cand != 0 ? 2 : 1);
@@ -180,6 +186,13 @@ cudaError_t launch_fill_fp32(int kind, const TraverseArgs &a, int grid, cudaStre
 cudaError_t launch_fill_fp64(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
                              const TravShape &shape);
 int occupancy_count_fp32(int kind, const TravShape &shape);
+// The FP32 instantiations that also take runs of home cells (TraverseArgs::runs).
+cudaError_t launch_count_fp32_runs(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                                   const TravShape &shape);
+cudaError_t launch_fill_fp32_runs(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+                                  const TravShape &shape);
+int occupancy_count_fp32_runs(int kind, const TravShape &shape);
+int occupancy_fill_fp32_runs(int kind, const TravShape &shape, bool lj);
 int occupancy_count_fp64(int kind, const TravShape &shape);
 int occupancy_fill_fp32(int kind, const TravShape &shape, bool lj);
 int occupancy_fill_fp64(int kind, const TravShape &shape, bool lj);

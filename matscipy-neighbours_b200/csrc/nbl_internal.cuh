@@ -109,15 +109,22 @@ struct HomeCell {
 
 // One work item of the pair passes, self-contained so that a warp needs one
 // 32-byte load to start it: the home cell (folded coordinates, system) and
-// the tile of its sorted atoms [ib, ib + nt).
+// the tile of its sorted atoms [ib, ib + nt).  A run (run > 1, dense grid
+// only) is `run` consecutive home cells along x starting at c, whose atoms
+// (contiguous in sorted order) form one tile; their neighbour cells are
+// visited once for the whole run.
 struct __align__(16) WorkItem {
     int32_t c[3];
     int32_t sys;
     int32_t ib;
     int32_t nt;
-    int32_t tidx;
-    int32_t pad;
+    int32_t tidx;  // table index of the (first) home cell
+    int32_t run;   // home cells in the item (1: a single cell)
 };
+
+// Home cells per run at most (and the bound on a run's x extent the FP32
+// guard band is sized for).
+constexpr int kMaxRun = 8;
 
 // Mask-pool reference of one (work item, segment batch), as the count stores
 // it: the first word in the low 40 bits, the batch's 32-candidate chunks per

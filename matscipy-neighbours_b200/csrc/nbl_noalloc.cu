@@ -261,7 +261,8 @@ extern "C" NBL_API nbl_status nbl_neighbour_list_noalloc(const nbl_request *req,
     NA_CUDA(launch_gather(ga, s), "k_gather");
     int nsm_tiles = 148;
     cudaDeviceGetAttribute(&nsm_tiles, cudaDevAttrMultiProcessorCount, dev);
-    NA_CUDA(launch_tiles(home, small, table, items, small + 3, N, nsm_tiles, 32, s), "k_tiles");
+    NA_CUDA(launch_tiles(home, small, table, sys, items, small + 3, N, nsm_tiles, 32, 1, s),
+            "k_tiles");
 
     TraverseArgs ta{};
     ta.sys = sys;

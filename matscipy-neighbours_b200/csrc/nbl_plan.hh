@@ -90,7 +90,7 @@ constexpr int kAutoWaves = 2;
 struct CountKey {
     const void *ws_base, *pos, *per_atom, *types;
     int64_t natoms, table_size, mask_cap, pt_size, i_lo, i_hi;
-    int32_t nsys, grid, key_bits, fp32, kind, itile, nvisit_tab;
+    int32_t nsys, grid, key_bits, fp32, kind, itile, max_run, nvisit_tab;
     int32_t count_mult, count_warps, count_cand, count_group, count_tickets;
     CountKey() { std::memset(this, 0, sizeof(*this)); }
     bool operator==(const CountKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
@@ -114,6 +114,10 @@ struct Plan {
     TravShape count_shape;
     TravShape fill_shape = default_fill_shape();
     int itile = 32;
+    // Home cells per work item at most (0: chosen on the device from the
+    // cells' mean occupancy; 1: one cell per item).  Runs of several cells
+    // are only built on the dense grid with the FP32 filter.
+    int max_run = 0;
     // Work items by atomic ticket (else a fixed warp stride) in each pass.
     bool count_tickets = true;
     bool fill_tickets = true;

@@ -1,6 +1,17 @@
 // nbl_trav_count32.cu -- the count pass with the FP32 filter, every launch
-// shape (warps per CTA x staged candidates x atoms per sweep x cutoff kind).
+// shape (warps per CTA x staged candidates x atoms per sweep x cutoff kind),
+// for one-cell work items.  nbl_trav_count32r.cu compiles the same file with
+// NBL_TRAV_RUNS = 1: the instantiations that also take runs of home cells.
 #include "nbl_traverse.cuh"
+
+#ifndef NBL_TRAV_RUNS
+#define NBL_TRAV_RUNS 0
+#endif
+#if NBL_TRAV_RUNS
+#define NBL_TRAV_NAME(x) x##_runs
+#else
+#define NBL_TRAV_NAME(x) x
+#endif
 
 namespace nbl {
 namespace {
@@ -8,7 +19,7 @@ namespace {
 template <int K, int G, int W, int C>
 TravKernel pick(size_t &smem) {
     smem = count_smem_bytes<true, C>(W);
-    return k_count<true, K, G, W, C>;
+    return k_count<true, K, G, W, C, NBL_TRAV_RUNS != 0>;
 }
 
 template <int K, int W>
@@ -33,14 +44,14 @@ TravKernel kernel_for(int kind, const TravShape &s, size_t &smem) {
 
 }  // namespace
 
-cudaError_t launch_count_fp32(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
+cudaError_t NBL_TRAV_NAME(launch_count_fp32)(int kind, const TraverseArgs &a, int grid, cudaStream_t st,
                               const TravShape &shape) {
     size_t smem = 0;
     const TravKernel k = kernel_for(kind, shape, smem);
     return launch_kernel(k, smem, shape.warps, a, grid, st);
 }
 
-int occupancy_count_fp32(int kind, const TravShape &shape) {
+int NBL_TRAV_NAME(occupancy_count_fp32)(int kind, const TravShape &shape) {
     size_t smem = 0;
     const TravKernel k = kernel_for(kind, shape, smem);
     return occupancy_kernel(k, smem, shape.warps);

@@ -8,7 +8,7 @@ namespace {
 template <int K, int W, int C>
 TravKernel pick(size_t &smem) {
     smem = count_smem_bytes<false, C>(W);
-    return k_count<false, K, 4, W, C>;
+    return k_count<false, K, 4, W, C, false>;
 }
 
 template <int K, int W>

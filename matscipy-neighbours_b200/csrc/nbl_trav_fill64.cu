@@ -10,10 +10,10 @@ template <int K, int W>
 TravKernel pick_w(bool lj, bool all5, size_t &smem) {
     if (lj) {
         smem = fill_smem_bytes<false>(4, true);
-        return k_fill<false, K, true, false, 4>;
+        return k_fill<false, K, true, false, 4, false>;
     }
     smem = fill_smem_bytes<false>(W, false);
-    return k_fill<false, K, false, false, W>;
+    return k_fill<false, K, false, false, W, false>;
 }
 
 template <int K>

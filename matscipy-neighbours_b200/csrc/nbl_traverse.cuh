@@ -91,6 +91,8 @@ struct SegSmem {
     float off32[kSeg][3];
     int32_t b[kSeg];
     int32_t pref[kSeg + 1];
+    int8_t xo[kSeg];    // runs: the segment's x cell offset from the run's first cell
+    uint8_t row[kSeg];  // runs: its (z, y) offset row, (dz + 1) * 3 + dy + 1
 };
 
 // A segment record's values (offset vector and image shift) in registers.
@@ -119,7 +121,10 @@ struct __align__(16) CountSmem {
     int32_t iatom[kITile];
     int32_t isi[kITile];       // sorted index of each (in-range) atom of the tile
     int32_t icount[kITile];
+    int8_t ht[kITile];         // runs: each atom's home cell within the run
 };
+static_assert(6 * (4 * sizeof(CountSmem<true, 384>) + 1024) <= 233472,
+              "six 4-warp count CTAs per SM fit the SM's shared memory");
 
 constexpr int kCandTab = 1024;   // candidates with a segment-table entry (fill)
 constexpr int kPosTab = 640;     // pairs per window with a position table (fill)
@@ -143,6 +148,7 @@ struct __align__(16) FillSmem {
         CandT<FP32> cand[FillTile<FP32>::kCand];  // staged candidates (recomputed words)
     };
     uint8_t cand_seg[kCandTab];     // segment of each of the batch's first candidates
+    int8_t ht[kITile];              // runs: each atom's home cell within the run
 };
 static_assert(5 * (4 * sizeof(FillSmem<true>) + 4 * 32 * 32 + 1024) <= 233472 &&
                   5 * (4 * sizeof(FillSmem<false>) + 4 * 32 * 32 + 1024) <= 233472,
@@ -156,30 +162,43 @@ struct Hot {
     int pbc_bits;
     int ncut;
     int pt_base;
+    int vrun;  // runs: the system's first visit-table entry; -1: a single cell
     int64_t atom_base;
 };
 
 struct Home {
-    int32_t cc[3];  // folded coordinates of the home cell
+    int32_t cc[3];  // folded coordinates of the (first) home cell
     int sys;
     const SysDev *S;
     Hot H;
     int nvisit;
+    int run;        // home cells of the item
 };
 
-template <bool FP32>
+// RUN: the kernel instantiation that takes runs (items of several home
+// cells); without it every item is one cell and the run code folds away.
+template <bool FP32, bool RUN>
 __device__ __forceinline__ Home load_home(const TraverseArgs &a, const WorkItem &w) {
     Home c;
+    const int run = RUN ? w.run : 1;
     c.cc[0] = w.c[0];
     c.cc[1] = w.c[1];
     c.cc[2] = w.c[2];
     c.sys = w.sys;
     c.S = a.sys + w.sys;
     const SysDev &S = *c.S;
+    c.H.vrun = run > 1 ? (int)S.visit_base : -1;
     c.H.lo_rc = c.H.hi_rc = c.H.band = 0.f;
     if (FP32) {
         const double R = S.cutoff;
-        const double M = 2.0 * (double)a.amax[w.sys] + S.off_max;
+        double M = 2.0 * (double)a.amax[w.sys] + S.off_max;
+        if (run > 1) {
+            // a run stages candidates and atoms in its first cell's frame:
+            // candidate offsets reach (run - 1) more cells along x, atom
+            // offsets up to run - 1 cells
+            const double bx = fmax(fabs(S.bin[0][0]), fmax(fabs(S.bin[0][1]), fabs(S.bin[0][2])));
+            M = dadd(M, dmul(2.0 * (double)(run - 1), bx) * (1.0 + 1e-12));
+        }
         const double band = guard_band(M, R);
         c.H.lo_rc = __double2float_rd(S.cutoff_sq - band);
         c.H.hi_rc = __double2float_ru(S.cutoff_sq + band);
@@ -190,7 +209,8 @@ __device__ __forceinline__ Home load_home(const TraverseArgs &a, const WorkItem 
     c.H.ncut = S.ncutoffs;
     c.H.pt_base = S.pt_base;
     c.H.atom_base = S.atom_base;
-    c.nvisit = S.nvisit;
+    c.run = run;
+    c.nvisit = run > 1 ? 9 * (run + 2) : S.nvisit;
     return c;
 }
 
@@ -223,7 +243,21 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
         int off3[3];
         double offd[3];
         float off32[3];
-        if (S.visit_base >= 0) {
+        uint8_t vrow = 0;
+        if (c.run > 1) {
+            // a run: rows (dz, dy) in the reference's order, each the run's
+            // cells plus one on either side, x ascending (so each atom sees its
+            // own 3 x 3 x 3 block in z/y/x order)
+            const int wr = c.run + 2;
+            const int xr = v % wr, rest = v / wr;
+            off3[0] = xr - 1;
+            off3[1] = rest % 3 - 1;
+            off3[2] = rest / 3 - 1;
+            vrow = (uint8_t)rest;
+            visit_offset(S, off3, offd);
+#pragma unroll
+            for (int k = 0; k < 3; k++) off32[k] = __double2float_rn(offd[k]);
+        } else if (S.visit_base >= 0) {
             const VisitDev &e = a.visit[S.visit_base + v];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -276,7 +310,11 @@ __device__ __forceinline__ void setup_segments(SegSmem &sg, const TraverseArgs &
             sg.off32[lane][k] = off32[k];
             sg.rec[lane].m[k] = m[k];
         }
-        zero = (off3[0] == 0 && off3[1] == 0 && off3[2] == 0);
+        if (c.run > 1) {
+            sg.xo[lane] = (int8_t)off3[0];
+            sg.row[lane] = vrow;
+        }
+        zero = c.run == 1 && off3[0] == 0 && off3[1] == 0 && off3[2] == 0;
     }
     int incl = len;
 #pragma unroll
@@ -408,14 +446,59 @@ __device__ __forceinline__ bool exact_inside(const Hot &H, const TraverseArgs &a
 }
 
 // Guard-band candidate kk of the batch for atom si, decided in FP64 (cold).
-template <int KIND>
+// In a run (H.vrun >= 0) the atom (home cell t of the run) only has the
+// segments within one cell of its own along x, with the offset vector of its
+// own cell offset (the reference's visit of that home cell).
+template <int KIND, bool RUN>
 __device__ __noinline__ bool resolve_exact(const SegSmem &sg, const TraverseArgs &a,
-                                           const Hot &H, int nseg, int kk, int si,
-                                           float wi) {
+                                           const Hot &H, const SysDev *S, int nseg, int kk,
+                                           int si, float wi, int t) {
     const int seg = seg_of(sg, nseg, kk);
     const int32_t sj = sg.b[seg] + (kk - sg.pref[seg]);
+    if (RUN && H.vrun >= 0) {
+        const int dx = (int)sg.xo[seg] - t;
+        if (dx < -1 || dx > 1) return false;
+        const int d[3] = {dx, (int)sg.row[seg] % 3 - 1, (int)sg.row[seg] / 3 - 1};
+        double off[3];
+        visit_offset(*S, d, off);
+        return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], off, wi, a.pos32[sj].w);
+    }
     return exact_inside<KIND>(H, a, a.pos64[si], a.pos64[sj], sg.rec[seg].off, wi,
                               a.pos32[sj].w);
+}
+
+// Runs: the home cell (0 .. run - 1) of sorted atom si, found among the run's
+// cell slices (every lane takes part; lane t < run reads cell t's slice).
+__device__ __forceinline__ int run_home_of(const TraverseArgs &a, const WorkItem &w, int si,
+                                           int lane) {
+    int2 sl = make_int2(0, 0);
+    if (lane < w.run) sl = a.table[w.tidx + lane];
+    int t = 0;
+    for (int u = 0; u < w.run; u++) {
+        const int b = __shfl_sync(0xffffffffu, sl.x, u);
+        const int e = __shfl_sync(0xffffffffu, sl.y, u);
+        if (si >= b && si < e) t = u;
+    }
+    return t;
+}
+
+// Runs: (first candidate index - first sorted atom) of home cell t's own
+// segment (zero offset) if it is in the batch starting at segment vb, else
+// INT_MIN / 2 (so that kself + si stays negative).
+__device__ __forceinline__ int run_self_base(const SegSmem &sg, int run, int vb, int nseg,
+                                             int t) {
+    const int zv = 4 * (run + 2) + t + 1 - vb;  // row (0, 0), x offset t
+    return (zv >= 0 && zv < nseg) ? sg.pref[zv] - sg.b[zv] : INT_MIN / 2;
+}
+
+// Runs: FP32 offset of home cell t from the run's first cell (the frame the
+// run's candidates and atoms are staged in).
+__device__ __forceinline__ float3 run_frame32(const SysDev &S, int t) {
+    const int d[3] = {t, 0, 0};
+    double o[3];
+    visit_offset(S, d, o);
+    return make_float3(__double2float_rn(o[0]), __double2float_rn(o[1]),
+                       __double2float_rn(o[2]));
 }
 
 // FP32 thresholds for one (atom, candidate) pair.
@@ -441,12 +524,13 @@ __device__ __forceinline__ void thresholds(const Hot &H, const TraverseArgs &a, 
 
 // Hit mask of one staged 32-candidate chunk (tile positions k0..k0+31) for one
 // atom: FP32 filter + FP64 guard band, or plain FP64.
-template <bool FP32, int KIND>
+template <bool FP32, int KIND, bool RUN>
 __device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const SegSmem &sg,
                                                const TraverseArgs &a, const Hot &H,
-                                               int nseg, int kb, int k0, int lane,
-                                               int kself_tile, int si, const float4 &pi32,
-                                               const double4 &pi64) {
+                                               const SysDev *S, int nseg, int kb, int k0,
+                                               int lane, int kself_tile, int si,
+                                               const float4 &pi32, const double4 &pi64,
+                                               int t) {
     const unsigned full = 0xffffffffu;
     const int k = k0 + lane;
     const bool notself = k != kself_tile;
@@ -462,7 +546,7 @@ __device__ __forceinline__ unsigned chunk_mask(const CandT<FP32> *cand, const Se
         const bool amb = !(r2 < lo) && (r2 < hi) && notself;
         if (__any_sync(full, amb)) {
             bool h2 = false;
-            if (amb) h2 = resolve_exact<KIND>(sg, a, H, nseg, kb + k, si, pi32.w);
+            if (amb) h2 = resolve_exact<KIND, RUN>(sg, a, H, S, nseg, kb + k, si, pi32.w, t);
             mask |= __ballot_sync(full, h2);
         }
         return mask;
@@ -578,7 +662,7 @@ __device__ __forceinline__ int div_small(int w, int n, float inv_n) {
 
 }  // namespace
 
-template <bool FP32, int KIND, int GROUP, int WARPS, int CAND>
+template <bool FP32, int KIND, int GROUP, int WARPS, int CAND, bool RUN>
 __global__ void __launch_bounds__(WARPS * 32, count_min_blocks(WARPS))
 k_count(TraverseArgs a) {
     constexpr int kCand = CAND;
@@ -596,7 +680,7 @@ k_count(TraverseArgs a) {
     while (L.it < nitems) {
         L.prefetch(a, nwarps, nitems, lane, false);
         const int it = L.it;
-        const Home c = load_home<FP32>(a, L.rec);
+        const Home c = load_home<FP32, RUN>(a, L.rec);
         const Hot &H = c.H;
         long long mbase = -1;
 
@@ -606,7 +690,9 @@ k_count(TraverseArgs a) {
             // The tile's atoms whose original index lies in [i_lo, i_hi),
             // compacted in order (all of them unless the rows are split); with
             // all rows they are copied asynchronously and land during the
-            // segment set-up.
+            // segment set-up.  In a run, each atom's home cell and FP32 frame
+            // offset (its cell's offset from the run's first cell).
+            const int t_l = c.run > 1 ? run_home_of(a, L.rec, ib + lane, lane) : 0;
             int ni;
             if (all_rows) {
                 ni = L.rec.nt;
@@ -615,6 +701,7 @@ k_count(TraverseArgs a) {
                     cp_async4(&sm.iatom[lane], &a.aux[ib + lane].x);
                     sm.isi[lane] = ib + lane;
                     sm.icount[lane] = 0;
+                    if (RUN) sm.ht[lane] = (int8_t)t_l;
                 }
             } else {
                 const int nt = L.rec.nt;
@@ -628,10 +715,18 @@ k_count(TraverseArgs a) {
                 ni = __popc(im);
                 if (in) {
                     const int c2 = __popc(im & lanemask_lt());
-                    sm.i32[c2] = a.pos32[ib + lane];
+                    float4 p = a.pos32[ib + lane];
+                    if (c.run > 1) {
+                        const float3 fo = run_frame32(*c.S, t_l);
+                        p.x += fo.x;
+                        p.y += fo.y;
+                        p.z += fo.z;
+                    }
+                    sm.i32[c2] = p;
                     sm.iatom[c2] = ax;
                     sm.isi[c2] = ib + lane;
                     sm.icount[c2] = 0;
+                    sm.ht[c2] = (int8_t)t_l;
                 }
                 __syncwarp();
             }
@@ -641,6 +736,17 @@ k_count(TraverseArgs a) {
                 setup_segments(sm.sg, a, c, vb, lane, nseg, total, zs);
                 cp_async_wait();
                 __syncwarp();
+                if (c.run > 1 && all_rows && vb == 0) {  // the copied atoms into the run's frame
+                    if (lane < ni) {
+                        const float3 fo = run_frame32(*c.S, sm.ht[lane]);
+                        float4 p = sm.i32[lane];
+                        p.x += fo.x;
+                        p.y += fo.y;
+                        p.z += fo.z;
+                        sm.i32[lane] = p;
+                    }
+                    __syncwarp();
+                }
                 const int nchunks_all = (total + 31) >> 5;
                 // One word region per (work item, segment batch): (atoms of the
                 // i-tile) x (chunks of the batch's candidate list).
@@ -681,7 +787,11 @@ k_count(TraverseArgs a) {
                                 const bool v = g0 + g < ni;
                                 pg[g] = v ? sm.i32[g0 + g]
                                           : make_float4(kFarAtom, kFarAtom, kFarAtom, 0.f);
-                                ks[g] = v ? kself0 + sm.isi[g0 + g] - kb : -1;
+                                const int ks0 = c.run == 1
+                                                    ? kself0
+                                                    : run_self_base(sm.sg, c.run, vb, nseg,
+                                                                    v ? sm.ht[g0 + g] : 0);
+                                ks[g] = v ? ks0 + sm.isi[g0 + g] - kb : -1;
                                 cnt[g] = 0;
                                 mw[g] = 0u;
                             }
@@ -747,9 +857,10 @@ k_count(TraverseArgs a) {
                                         for (int g = 0; g < GROUP; g++) {
                                             bool h2 = false;
                                             if (amb[g])
-                                                h2 = resolve_exact<KIND>(sm.sg, a, H, nseg,
-                                                                         kb + k, sm.isi[g0 + g],
-                                                                         pg[g].w);
+                                                h2 = resolve_exact<KIND, RUN>(
+                                                    sm.sg, a, H, RUN ? c.S : nullptr, nseg,
+                                                    kb + k, sm.isi[g0 + g], pg[g].w,
+                                                    RUN ? (int)sm.ht[g0 + g] : 0);
                                             m[g] |= __ballot_sync(full, h2);
                                         }
                                     }
@@ -797,9 +908,9 @@ k_count(TraverseArgs a) {
                             int cnt = 0;
                             unsigned mword = 0;
                             for (int ch = 0; ch < nck; ch++) {
-                                const unsigned mask = chunk_mask<FP32, KIND>(
-                                    sm.cand, sm.sg, a, H, nseg, kb, ch * 32, lane, kself_tile,
-                                    si, pi32, pi64);
+                                const unsigned mask = chunk_mask<FP32, KIND, RUN>(
+                                    sm.cand, sm.sg, a, H, RUN ? c.S : nullptr, nseg, kb, ch * 32, lane,
+                                    kself_tile, si, pi32, pi64, 0);
                                 cnt += __popc(mask);
                                 mword = (lane == (ch & 31)) ? mask : mword;
                                 if (mbase >= 0 && ((ch & 31) == 31 || ch == nck - 1)) {
@@ -883,11 +994,33 @@ __device__ __forceinline__ PairWork fetch_pair(const FillSmem<FP32> &sm,
     return w;
 }
 
+// A pair's segment values: the segment's own offset vector (single-cell
+// items) or, in a run, the one of the pair's cell offset from atom il's own
+// home cell (entry v of the system's 27 visited offsets, z/y/x order).
+template <bool FP32, bool RUN>
+__device__ __forceinline__ SegVals pair_seg_vals(const FillSmem<FP32> &sm,
+                                                 const TraverseArgs &a, const Hot &H, int seg,
+                                                 int il) {
+    SegVals g = seg_vals(sm.sg.rec[seg]);
+    if (RUN && H.vrun >= 0) {
+        // hits lie within one cell of the atom's own along x, so v < 27;
+        // the clamp only keeps the table read in bounds
+        int v = (int)sm.sg.row[seg] * 3 + ((int)sm.sg.xo[seg] - (int)sm.ht[il] + 1);
+        checked_fail(v < 0 || v >= 27, a.err);
+        v = min(max(v, 0), 26);
+        const double *o = a.visit[H.vrun + v].off;
+        g.o0 = o[0];
+        g.o1 = o[1];
+        g.o2 = o[2];
+    }
+    return g;
+}
+
 // Compute and store one pair (exact FP64 D and d, S, i, j).  ALL5: all five
 // outputs requested and no neighbour matrix (no per-pair output checks).
 // check: test the slot against the output capacity (warp-uniform; false when
 // the whole list is known to fit).
-template <bool FP32, bool ALL5>
+template <bool FP32, bool ALL5, bool RUN>
 __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const TraverseArgs &a,
                                            const Hot &H, const PairWork &w, bool check) {
     if (!w.act) return;
@@ -900,7 +1033,7 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
                          a.err))
             return;
     }
-    const SegVals g = seg_vals(sm.sg.rec[w.seg]);
+    const SegVals g = pair_seg_vals<FP32, RUN>(sm, a, H, w.seg, w.il);
     const double dx = dadd(dsub(w.pj.x, pi.x), g.o0);
     const double dy = dadd(dsub(w.pj.y, pi.y), g.o1);
     const double dz = dadd(dsub(w.pj.z, pi.z), g.o2);
@@ -949,16 +1082,16 @@ __device__ __forceinline__ void store_pair(const FillSmem<FP32> &sm, const Trave
 // lanes' forces and energy shares (1/2 U per directed pair) are summed per
 // atom (runs of equal i are contiguous) and the run's last lane adds them to
 // the tile's shared-memory sums.
-template <bool FP32>
+template <bool FP32, bool RUN>
 __device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc)[4],
-                                         const TraverseArgs &a, const PairWork &w, int lane) {
+                                         const TraverseArgs &a, const Hot &H, const PairWork &w,
+                                         int lane) {
     const unsigned full = 0xffffffffu;
     double f0 = 0.0, f1 = 0.0, f2 = 0.0, e = 0.0;
     const int il = w.act ? w.il : -1;
     if (w.act) {
         const double4 pi = sm.i64[w.il];
-        const int seg = w.seg;
-        const SegVals g = seg_vals(sm.sg.rec[seg]);
+        const SegVals g = pair_seg_vals<FP32, RUN>(sm, a, H, w.seg, w.il);
         const double dx = dadd(dsub(w.pj.x, pi.x), g.o0);
         const double dy = dadd(dsub(w.pj.y, pi.y), g.o1);
         const double dz = dadd(dsub(w.pj.z, pi.z), g.o2);
@@ -996,7 +1129,7 @@ __device__ __forceinline__ void lj_round(const FillSmem<FP32> &sm, double (*facc
     __syncwarp();
 }
 
-template <bool FP32, int KIND, bool LJ, bool ALL5, int WARPS>
+template <bool FP32, int KIND, bool LJ, bool ALL5, int WARPS, bool RUN>
 __global__ void __launch_bounds__(WARPS * 32, fill_min_blocks(WARPS))
 k_fill(TraverseArgs a) {
     constexpr int kCand = FillTile<FP32>::kCand;
@@ -1020,13 +1153,17 @@ k_fill(TraverseArgs a) {
     while (L.it < nitems) {
         L.prefetch(a, nwarps, nitems, lane, true);
         const int it = L.it;
-        const Home c = load_home<FP32>(a, L.rec);
+        const Home c = load_home<FP32, RUN>(a, L.rec);
         const Hot &H = c.H;
 
         do {
             const int ib = L.rec.ib;
             if (item_bad(a, L.rec)) break;
             int ni;
+            // A run: each atom's home cell (a pair's D uses the offset of its
+            // atom's own cell).
+            int t_l = 0;
+            if (c.run > 1) t_l = run_home_of(a, L.rec, ib + lane, lane);
             // The tile's atoms: with all rows copied asynchronously (they land
             // during the segment set-up; the row starts follow once their
             // indices are in), else the in-range ones compacted in order.
@@ -1041,6 +1178,7 @@ k_fill(TraverseArgs a) {
                     cp_async16(dst + 16, src + 16);
                     cp_async16(&sm.iaux[lane], &a.aux[ib + lane]);
                     sm.isi[lane] = ib + lane;
+                    sm.ht[lane] = (int8_t)t_l;
                     if (LJ) facc[lane][0] = facc[lane][1] = facc[lane][2] = facc[lane][3] = 0.0;
                 }
                 off_pending = true;
@@ -1060,6 +1198,7 @@ k_fill(TraverseArgs a) {
                     sm.i64[c2] = a.pos64[si];
                     sm.iaux[c2] = ax;
                     sm.isi[c2] = si;
+                    sm.ht[c2] = (int8_t)t_l;
                     sm.icur[c2] = checked_fail(ax.x >= a.natoms, a.err)
                                       ? 0ll
                                       : (long long)a.offsets[ax.x];
@@ -1130,13 +1269,22 @@ k_fill(TraverseArgs a) {
                                 stage_segs<FP32>(sm.cand, sm.sg, a, nseg, kr + kt, nk, nkp, lane);
                                 for (int al = 0; al < na; al++) {
                                     const int il = a0 + al, si = sm.isi[il];
-                                    const float4 pi32 = a.pos32[si];
+                                    float4 pi32 = a.pos32[si];
                                     const double4 pi64 = sm.i64[il];
-                                    const int kself_tile = kself0 + si - (kr + kt);
+                                    int ks0 = kself0;
+                                    if (c.run > 1) {  // the run's frame and the atom's own cell
+                                        const float3 fo = run_frame32(*c.S, sm.ht[il]);
+                                        pi32.x += fo.x;
+                                        pi32.y += fo.y;
+                                        pi32.z += fo.z;
+                                        ks0 = run_self_base(sm.sg, c.run, vb, nseg, sm.ht[il]);
+                                    }
+                                    const int kself_tile = ks0 + si - (kr + kt);
                                     for (int ch = 0; ch < (nkp >> 5); ch++) {
-                                        const unsigned mask = chunk_mask<FP32, KIND>(
-                                            sm.cand, sm.sg, a, H, nseg, kr + kt, ch * 32, lane,
-                                            kself_tile, si, pi32, pi64);
+                                        const unsigned mask = chunk_mask<FP32, KIND, RUN>(
+                                            sm.cand, sm.sg, a, H, RUN ? c.S : nullptr, nseg,
+                                            kr + kt, ch * 32, lane, kself_tile, si, pi32, pi64,
+                                            RUN ? (int)sm.ht[il] : 0);
                                         if (lane == 0) sm.mw[al * nch + (kt >> 5) + ch] = mask;
                                     }
                                 }
@@ -1205,9 +1353,9 @@ k_fill(TraverseArgs a) {
                                                                   nch, inv_nch, kr, a0, carry,
                                                                   P0 + 32 + lane, tab);
                             if (LJ)
-                                lj_round<FP32>(sm, facc, a, cur, lane);
+                                lj_round<FP32, RUN>(sm, facc, a, H, cur, lane);
                             else
-                                store_pair<FP32, ALL5>(sm, a, H, cur, !cap_ok);
+                                store_pair<FP32, ALL5, RUN>(sm, a, H, cur, !cap_ok);
                             cur = nxt;
                         }
                         __syncwarp();
