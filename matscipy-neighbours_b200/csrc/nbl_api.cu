@@ -472,57 +472,35 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
     return NBL_SUCCESS;
 }
 
-// Enqueue the count phase (bin, sort, gather, work items, count, scan) on a
-// batch whose inputs are resident: no host synchronisation, no allocation,
-// so it can be captured in a CUDA graph.
-nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
-    StageRange whole("nbl.count_phase");
-    Bufs &B = p.bufs;
-    const int64_t N = b.natoms;
-    const int nsys = (int)b.sys.size();
-    NBL_CUDA(launch_init(B.sys, nsys, B.visit, B.small, B.table, b.table_size, B.amax,
-                         b.grid == kGridHashed ? B.hkey : nullptr, p.num_sms, st),
-             "k_init");
-
-    int *n_home = B.small + 0;
-    int *err = B.small + 1;
-
-    BinArgs ba;
+// The argument blocks of the count phase's stages for batch b: binning,
+// gather (over the sorted keys / values), and the pair passes' (into
+// p.targs, with the passes' grids).
+static void bin_args(const Plan &p, const Batch &b, BinArgs &ba) {
+    const Bufs &B = p.bufs;
     ba.sys = B.sys;
     ba.sys_atom_base = B.sys_atom_base;
-    ba.nsys = nsys;
+    ba.nsys = (int)b.sys.size();
     ba.grid = b.grid;
     ba.positions = B.pos;
-    ba.natoms = N;
+    ba.natoms = b.natoms;
     ba.keys = B.keys;
     ba.vals = B.vals;
     ba.hkey = B.hkey;
     ba.hmask = (unsigned long long)(b.table_size - 1);
-    ba.err = err;
-    {
-        StageRange r("nbl.bin");
-        NBL_CUDA(launch_bin(ba, st), "k_bin");
-    }
+    ba.err = B.small + 1;
+}
 
-    bool in_alt = false;
-    {
-        StageRange r("nbl.sort");
-        NBL_CUDA(radix_sort_pairs(B.keys, B.vals, B.keys2, B.vals2, N, b.key_bits, B.hist,
-                                  B.hist_scan, B.scan32, st, &in_alt),
-                 "radix sort");
-    }
-    const uint32_t *skeys = in_alt ? B.keys2 : B.keys;
-    const int32_t *svals = in_alt ? B.vals2 : B.vals;
-
-    GatherArgs ga;
+static void gather_args(const Plan &p, const Batch &b, const uint32_t *skeys,
+                        const int32_t *svals, GatherArgs &ga) {
+    const Bufs &B = p.bufs;
     ga.sys = B.sys;
     ga.sys_atom_base = B.sys_atom_base;
-    ga.nsys = nsys;
+    ga.nsys = (int)b.sys.size();
     ga.grid = b.grid;
     ga.positions = B.pos;
     ga.per_atom = B.per_atom;
     ga.types = B.types;
-    ga.natoms = N;
+    ga.natoms = b.natoms;
     ga.keys = skeys;
     ga.vals = svals;
     ga.table = B.table;
@@ -531,21 +509,18 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ga.aux = B.aux;
     ga.amax = B.amax;
     ga.home = B.home;
-    ga.n_home = n_home;
-    {
-        StageRange r("nbl.gather");
-        NBL_CUDA(launch_gather(ga, st), "k_gather");
-        NBL_CUDA(launch_tiles(B.home, n_home, B.table, B.sys, B.items, B.small + 3, N,
-                              p.num_sms, p.itile, run_limit(p, b), st),
-                 "k_tiles");
-    }
+    ga.n_home = B.small + 0;
+}
 
+static void traverse_args(Plan &p, const Batch &b) {
+    const Bufs &B = p.bufs;
+    const int64_t N = b.natoms;
     TraverseArgs &ta = p.targs;
     std::memset(&ta, 0, sizeof(ta));
     ta.sys = B.sys;
     ta.visit = B.visit;
     ta.home = B.home;
-    ta.n_home = n_home;
+    ta.n_home = B.small + 0;
     ta.items = B.items;
     ta.n_items = B.small + 3;
     ta.grid = b.grid;
@@ -565,22 +540,58 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     ta.item_next = p.count_tickets ? B.small + 6 : nullptr;
     ta.mask_cap = B.mask_cap;
     ta.home_mask = B.home_mask;
-    ta.err = err;
+    ta.err = B.small + 1;
     ta.i_lo = p.i_lo;
     ta.i_hi = p.i_hi;
     ta.itile = p.itile;
     ta.natoms = N;
     ta.runs = run_limit(p, b) != 1 ? 1 : 0;
-    if (p.i_lo > 0 || p.i_hi < N)
-        NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
     p.trav_grid = traverse_grid(p, N, p.count_mult, kModeCount, b.fp32, p.batch_kind,
                                 p.count_shape, false);
     p.fill_grid = traverse_grid(p, N, p.fill_mult, kModeFill, b.fp32, p.batch_kind,
                                 p.fill_shape, false);
+}
+
+// Enqueue the count phase (bin, sort, gather, work items, count, scan) on a
+// batch whose inputs are resident: no host synchronisation, no allocation,
+// so it can be captured in a CUDA graph.
+nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
+    StageRange whole("nbl.count_phase");
+    Bufs &B = p.bufs;
+    const int64_t N = b.natoms;
+    const int nsys = (int)b.sys.size();
+    NBL_CUDA(launch_init(B.sys, nsys, B.visit, B.small, B.table, b.table_size, B.amax,
+                         b.grid == kGridHashed ? B.hkey : nullptr, p.num_sms, st),
+             "k_init");
+    BinArgs ba;
+    bin_args(p, b, ba);
+    {
+        StageRange r("nbl.bin");
+        NBL_CUDA(launch_bin(ba, st), "k_bin");
+    }
+    bool in_alt = false;
+    {
+        StageRange r("nbl.sort");
+        NBL_CUDA(radix_sort_pairs(B.keys, B.vals, B.keys2, B.vals2, N, b.key_bits, B.hist,
+                                  B.hist_scan, B.scan32, st, &in_alt),
+                 "radix sort");
+    }
+    GatherArgs ga;
+    gather_args(p, b, in_alt ? B.keys2 : B.keys, in_alt ? B.vals2 : B.vals, ga);
+    {
+        StageRange r("nbl.gather");
+        NBL_CUDA(launch_gather(ga, st), "k_gather");
+        NBL_CUDA(launch_tiles(B.home, ga.n_home, B.table, B.sys, B.items, B.small + 3, N,
+                              p.num_sms, p.itile, run_limit(p, b), st),
+                 "k_tiles");
+    }
+    traverse_args(p, b);
+    if (p.i_lo > 0 || p.i_hi < N)
+        NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     {
         StageRange r("nbl.count");
-        TraverseArgs tc = ta;
+        TraverseArgs tc = p.targs;
         tc.ticket_ready = 1;  // k_init cleared the ticket
         NBL_CUDA(launch_traverse(kModeCount, b.fp32, p.batch_kind, tc, p.trav_grid, st,
                                  p.count_shape),
@@ -590,6 +601,35 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
         StageRange r("nbl.scan");
         NBL_CUDA(exclusive_scan_i32_i64(B.counts, N, B.offsets, B.scan64, st), "scan");
     }
+    return NBL_SUCCESS;
+}
+
+// Whether batch b takes the one-CTA count phase (nbl_small.cu): one system of
+// up to p.small_atoms atoms on a dense grid of at most kSmallMaxCells cells,
+// every row.
+static bool small_path(const Plan &p, const Batch &b) {
+    return p.small_atoms > 0 && b.sys.size() == 1 && b.natoms >= 1 &&
+           b.natoms <= std::min<int64_t>(p.small_atoms, kSmallMaxAtoms) &&
+           b.grid == kGridDense && b.table_size <= kSmallMaxCells && p.i_lo <= 0 &&
+           p.i_hi >= b.natoms;
+}
+
+// The count phase of a small system as one launch: the same buffers as
+// enqueue_count leaves (the fill and the other consumers follow unchanged).
+static nbl_status enqueue_count_small(Plan &p, const Batch &b, cudaStream_t st) {
+    StageRange whole("nbl.count_phase");
+    Bufs &B = p.bufs;
+    SmallCountArgs sa;
+    bin_args(p, b, sa.bin);
+    gather_args(p, b, B.keys, B.vals, sa.gather);
+    traverse_args(p, b);
+    sa.trav = p.targs;
+    sa.trav.item_next = p.count_tickets ? B.small + 6 : nullptr;
+    sa.ncells = b.table_size;
+    sa.small = B.small;
+    sa.items_count = B.small + 3;
+    sa.offsets = B.offsets;
+    NBL_CUDA(launch_count_small(b.fp32, p.batch_kind, sa, st), "one-CTA count phase");
     return NBL_SUCCESS;
 }
 
@@ -670,10 +710,12 @@ static bool capture_count(Plan &p, const Batch &b, const CountKey &k) {
 nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
     nbl_status s = upload_batch(p, b, st);
     if (s != NBL_SUCCESS) return s;
+    const bool small = sync && small_path(p, b);
     // Single calls: replay the captured count phase while the launch key
-    // repeats (captured on the second call with the same key).
+    // repeats (captured on the second call with the same key); a small
+    // system's count phase is one launch already.
     bool replay = false;
-    if (sync && !p.graphs_off) {
+    if (sync && !small && !p.graphs_off) {
         const CountKey k = count_key(p, b);
         if (p.count_graph && k == p.graph_key) {
             replay = true;
@@ -697,7 +739,7 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
         NBL_CUDA(cudaGraphLaunch(p.count_graph, st), "count-phase graph");
         count_launch((int)p.graph_launches);
     } else {
-        s = enqueue_count(p, b, st);
+        s = small ? enqueue_count_small(p, b, st) : enqueue_count(p, b, st);
         if (s != NBL_SUCCESS) return s;
     }
     Bufs &B = p.bufs;
@@ -743,10 +785,14 @@ nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_
     return NBL_SUCCESS;
 }
 
-nbl_status read_flags(Plan &p, cudaStream_t st) {
-    NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, p.bufs.small, sizeof(int) * 2,
-                             cudaMemcpyDeviceToHost, st), "read flags");
-    NBL_CUDA(cudaStreamSynchronize(st), "check");
+// The device flags of the last count / fill as a status; with `copy`, first
+// reads them (synchronising `st`), else they were read already.
+nbl_status read_flags(Plan &p, cudaStream_t st, bool copy) {
+    if (copy) {
+        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, p.bufs.small, sizeof(int) * 2,
+                                 cudaMemcpyDeviceToHost, st), "read flags");
+        NBL_CUDA(cudaStreamSynchronize(st), "check");
+    }
     int flags[2];
     std::memcpy(flags, p.host_small + 1, sizeof(flags));
     if (flags[1] & kErrRange)
@@ -771,6 +817,9 @@ void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
     cfg->count_large_staging = p.count_shape.cand;
     cfg->atoms_per_item = p.itile;
     cfg->cells_per_item = p.max_run;
+    cfg->single_cta_atoms = p.small_atoms == kSmallDefaultAtoms ? 0
+                            : p.small_atoms > 0                ? p.small_atoms
+                                                               : -1;
 }
 
 // Request -> one-system batch.
@@ -868,9 +917,12 @@ void plan_free(Plan &p) {
     p.ws.release();
     if (p.host_small) cudaFreeHost(p.host_small);
     if (p.host_stage) cudaFreeHost(p.host_stage);
+    if (p.host_out) cudaFreeHost(p.host_out);
     if (p.stage_done) cudaEventDestroy(p.stage_done);
     p.host_small = nullptr;
     p.host_stage = nullptr;
+    p.host_out = nullptr;
+    p.host_out_bytes = 0;
     p.stage_done = nullptr;
 }
 
@@ -971,12 +1023,14 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     const int itile = cfg->atoms_per_item == 0 ? 32 : cfg->atoms_per_item;
     if (cfg->count_ctas_per_sm < 0 || cfg->count_ctas_per_sm > 64 || cfg->fill_ctas_per_sm < 0 ||
         cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 || cfg->cells_per_item < 0 ||
-        cfg->cells_per_item > kMaxRun || !traverse_shape_ok(kModeCount, true, cs) ||
+        cfg->cells_per_item > kMaxRun || cfg->single_cta_atoms < -1 ||
+        cfg->single_cta_atoms > kSmallMaxAtoms || !traverse_shape_ok(kModeCount, true, cs) ||
         !traverse_shape_ok(kModeFill, true, fs))
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "launch config: CTAs per SM in [0, 64], warps 2, 4 or 8, count group "
                          "2 or 4, large candidate staging 0 or 1, atoms per item in [1, 32], "
-                         "cells per item in [0, %d]", kMaxRun);
+                         "cells per item in [0, %d], single-CTA atoms in [-1, %d]", kMaxRun,
+                         kSmallMaxAtoms);
     plan->p.count_mult = cfg->count_ctas_per_sm;
     plan->p.fill_mult = cfg->fill_ctas_per_sm;
     plan->p.count_tickets = cfg->count_strided == 0;
@@ -985,6 +1039,9 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     plan->p.fill_shape = fs;
     plan->p.itile = itile;
     plan->p.max_run = cfg->cells_per_item;
+    plan->p.small_atoms = cfg->single_cta_atoms == 0   ? kSmallDefaultAtoms
+                          : cfg->single_cta_atoms < 0 ? 0
+                                                      : cfg->single_cta_atoms;
     return NBL_SUCCESS;
 }
 
@@ -1052,6 +1109,31 @@ nbl_status nbl_fill_host(nbl_plan *plan, const nbl_outputs *host_out, void *stre
     d.shift = h.shift ? (int32_t *)(base + o_S) : nullptr;
     s = run_fill(p, d, np, st);
     if (s != NBL_SUCCESS) return s;
+    // Small lists: one copy of the contiguous outputs (and the flags) into the
+    // plan's pinned landing area, then host copies into the caller's arrays --
+    // cheaper than one device->host copy per quantity below a few hundred KB.
+    constexpr size_t kOneCopyBytes = 256 << 10;
+    if (L.total <= kOneCopyBytes) {
+        if (L.total > p.host_out_bytes) {
+            if (p.host_out) cudaFreeHost(p.host_out);
+            p.host_out = nullptr;
+            p.host_out_bytes = 0;
+            NBL_CUDA(cudaMallocHost(&p.host_out, kOneCopyBytes), "pinned landing area");
+            p.host_out_bytes = kOneCopyBytes;
+        }
+        NBL_CUDA(cudaMemcpyAsync(p.host_out, base, L.total, cudaMemcpyDeviceToHost, st),
+                 "copy outputs");
+        NBL_CUDA(cudaMemcpyAsync(p.host_small + 1, p.bufs.small, sizeof(int) * 2,
+                                 cudaMemcpyDeviceToHost, st), "read flags");
+        NBL_CUDA(cudaStreamSynchronize(st), "fill");
+        const char *hb = static_cast<const char *>(p.host_out);
+        if (h.first) std::memcpy(h.first, hb + o_i, sizeof(int32_t) * np);
+        if (h.second) std::memcpy(h.second, hb + o_j, sizeof(int32_t) * np);
+        if (h.distvec) std::memcpy(h.distvec, hb + o_D, sizeof(double) * 3 * np);
+        if (h.absdist) std::memcpy(h.absdist, hb + o_d, sizeof(double) * np);
+        if (h.shift) std::memcpy(h.shift, hb + o_S, sizeof(int32_t) * 3 * np);
+        return read_flags(p, st, false);
+    }
     if (h.first)
         NBL_CUDA(cudaMemcpyAsync(h.first, d.first, sizeof(int32_t) * np,
                                  cudaMemcpyDeviceToHost, st), "copy i");

@@ -147,6 +147,25 @@ constexpr int kMaskBatches = 4;
 cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, double *out,
                              cudaStream_t st);
 
+// The whole count phase of one small system in one CTA (nbl_small.cu): init,
+// bin, a stable sort in shared memory, gather, work items, the count pass and
+// the row offsets, leaving the same buffers as the multi-kernel sequence.
+// Dense grid, one system, 1..kSmallMaxAtoms atoms (by default systems of up
+// to kSmallDefaultAtoms take it), at most kSmallMaxCells cells, every row.
+constexpr int kSmallMaxAtoms = 2048;
+constexpr int kSmallDefaultAtoms = 256;
+constexpr int64_t kSmallMaxCells = 16384;
+struct SmallCountArgs {
+    BinArgs bin;          // keys / vals: sorted in place
+    GatherArgs gather;    // keys / vals: the same arrays
+    TraverseArgs trav;    // the count pass (and, unchanged, the fill after it)
+    int64_t ncells;       // cell-table entries to clear
+    int *small;           // the 8-int flag block
+    int *items_count;     // == trav.n_items
+    int64_t *offsets;     // [natoms + 1]
+};
+cudaError_t launch_count_small(bool fp32, int kind, const SmallCountArgs &a, cudaStream_t st);
+
 // Fill the visit tables of the systems that have one (visit_base >= 0).
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
 // Start of a count phase in one launch: zero the 8-int flag block, the cell

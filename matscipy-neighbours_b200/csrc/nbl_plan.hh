@@ -118,6 +118,9 @@ struct Plan {
     // cells' mean occupancy; 1: one cell per item).  Runs of several cells
     // are only built on the dense grid with the FP32 filter.
     int max_run = 0;
+    // Systems of up to this many atoms (at most kSmallMaxAtoms) take the
+    // one-CTA count phase; 0: never.
+    int small_atoms = kSmallDefaultAtoms;
     // Work items by atomic ticket (else a fixed warp stride) in each pass.
     bool count_tickets = true;
     bool fill_tickets = true;
@@ -136,6 +139,8 @@ struct Plan {
     int64_t *host_small = nullptr;  // pinned: [0] pair count, [1] flags
     void *host_stage = nullptr;     // pinned staging of the small host tables
     size_t host_stage_bytes = 0;
+    void *host_out = nullptr;       // pinned landing area of small host fills
+    size_t host_out_bytes = 0;
     cudaEvent_t stage_done = nullptr;
     bool stage_in_flight = false;
     // Count-phase graph of the single-call path (see CountKey).
@@ -176,7 +181,9 @@ nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st);
 nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st);
 nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync);
 nbl_status run_fill(Plan &p, const nbl_outputs &o, int64_t capacity, cudaStream_t st);
-nbl_status read_flags(Plan &p, cudaStream_t st);
+// The device flags of the last count / fill as a status (copy: read them
+// first, synchronising st).
+nbl_status read_flags(Plan &p, cudaStream_t st, bool copy = true);
 void launch_config_of(const Plan &p, nbl_launch_config *cfg);
 
 }  // namespace nbl

@@ -662,18 +662,18 @@ __device__ __forceinline__ int div_small(int w, int n, float inv_n) {
 
 }  // namespace
 
-template <bool FP32, int KIND, int GROUP, int WARPS, int CAND, bool RUN>
-__global__ void __launch_bounds__(WARPS * 32, count_min_blocks(WARPS))
-k_count(TraverseArgs a) {
+// The count pass for one warp of the calling CTA: global warp `gwarp` of
+// `nwarps` takes work items (by ticket, else at that stride); `smem_base` is
+// the CTA's per-warp count state (one CountSmem per warp of the CTA).
+template <bool FP32, int KIND, int GROUP, int CAND, bool RUN>
+__device__ __forceinline__ void count_items(const TraverseArgs &a, unsigned char *smem_base,
+                                            int gwarp, int nwarps) {
     constexpr int kCand = CAND;
-    constexpr int kWarps = WARPS;
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    CountSmem<FP32, CAND> *smem = reinterpret_cast<CountSmem<FP32, CAND> *>(dyn_smem);
+    CountSmem<FP32, CAND> *smem = reinterpret_cast<CountSmem<FP32, CAND> *>(smem_base);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CountSmem<FP32, CAND> &sm = smem[warp];
     const unsigned full = 0xffffffffu;
     const int nitems = *a.n_items;
-    const int gwarp = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
 
     const bool all_rows = all_rows_of(a);
     ItemLoop L(a, gwarp, nitems, lane, false);
@@ -933,6 +933,15 @@ k_count(TraverseArgs a) {
         } while (0);
         L.step();
     }
+}
+
+template <bool FP32, int KIND, int GROUP, int WARPS, int CAND, bool RUN>
+__global__ void __launch_bounds__(WARPS * 32, count_min_blocks(WARPS))
+k_count(TraverseArgs a) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5;
+    count_items<FP32, KIND, GROUP, CAND, RUN>(a, dyn_smem, blockIdx.x * WARPS + warp,
+                                              gridDim.x * WARPS);
 }
 
 // Segment of candidate kk of the batch: from the table, else by search.

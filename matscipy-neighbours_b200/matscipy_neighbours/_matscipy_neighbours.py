@@ -81,7 +81,7 @@ class LaunchConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "count_ctas_per_sm", "fill_ctas_per_sm", "count_strided", "fill_strided",
         "count_warps", "fill_warps", "count_group", "count_large_staging",
-        "atoms_per_item", "cells_per_item")]
+        "atoms_per_item", "cells_per_item", "single_cta_atoms")]
 
     def as_dict(self):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
@@ -311,11 +311,24 @@ _SHAPES = {"i": ((), np.int32), "j": ((), np.int32), "D": ((3,), np.float64),
            "d": ((), np.float64), "S": ((3,), np.int32)}
 
 
+# Below this many output bytes nbl_fill_host lands the whole list in the
+# plan's own pinned buffer with one copy and copies it on into the caller's
+# arrays, so plain numpy arrays are as fast as page-locked ones (and cheaper
+# to allocate).
+_ONE_COPY_BYTES = 256 << 10
+
+
+_PAIR_BYTES = {"i": 4, "j": 4, "D": 24, "d": 8, "S": 12}
+
+
 def _host_outputs(quantities, npairs):
+    kinds = set(quantities)
+    total = npairs * sum(_PAIR_BYTES[ch] for ch in kinds)
+    alloc = np.empty if total <= _ONE_COPY_BYTES else host_empty
     bufs = {}
-    for ch in set(quantities):
+    for ch in kinds:
         extra, dt = _SHAPES[ch]
-        bufs[ch] = host_empty((npairs,) + extra, dt)
+        bufs[ch] = alloc((npairs,) + extra, dt)
     return bufs
 
 

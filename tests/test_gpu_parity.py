@@ -1,6 +1,8 @@
 """GPU engine vs the CPU oracle: bit-identical outputs (same arrays, same
 order) for every precision mode and grid layout, on the reference's golden
-cases, the five workload shapes at reduced size, and edge cases."""
+cases, the five workload shapes at reduced size, and edge cases.  The golden
+and edge cases run through both count phases: the one-CTA launch that small
+systems take by default and the multi-kernel sequence (single-CTA path off)."""
 import itertools
 
 import numpy as np
@@ -23,6 +25,19 @@ def _restore_options():
     set_options(precision=prev["precision"], grid=prev["grid"])
 
 
+@pytest.fixture(params=["one_cta", "multi_kernel"])
+def count_path(request):
+    """The plan's single-CTA threshold: its largest value (every golden and
+    edge case that fits takes the one-CTA count phase), or -1 (never)."""
+    import ctypes
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    plan = ext.plan_for(0)
+    cfg = ext.LaunchConfig(single_cta_atoms=2048 if request.param == "one_cta" else -1)
+    ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
+    yield request.param
+    ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(ext.LaunchConfig())))
+
+
 def engine(q, w, precision="fp32", grid="auto"):
     import matscipy_neighbours as m
     from matscipy_neighbours import _matscipy_neighbours as ext
@@ -43,7 +58,7 @@ def expected(oracle, q, w):
 
 @pytest.mark.parametrize("mode", MODES, ids=["-".join(m) for m in MODES])
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
-def test_golden(case, mode):
+def test_golden(case, mode, count_path):
     out = engine(case["quantities"], case, *mode)
     if len(case["quantities"]) == 1:
         out = (out,)
@@ -147,7 +162,7 @@ EDGE = _edge_cases()
 
 @pytest.mark.parametrize("mode", MODES, ids=["-".join(m) for m in MODES])
 @pytest.mark.parametrize("name,w", EDGE, ids=[n for n, _ in EDGE])
-def test_edge_cases(oracle, name, w, mode):
+def test_edge_cases(oracle, name, w, mode, count_path):
     q = "ijdDS"
     assert_same_lists(engine(q, w, *mode), expected(oracle, q, w), q)
 
