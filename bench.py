@@ -651,6 +651,63 @@ def _cpu_fn(O, cores):
     return "port", 1, O.oracle_neighbour_list
 
 
+def per_call_latency(dev, sizes=(100, 1000), calls=60):
+    """Host-clock latency of one whole call on small systems (random gas,
+    0.08 atoms/A^3, rc 4 A, all five outputs): through the C-ABI with device
+    positions and device outputs (nbl_count + nbl_fill, then a stream
+    synchronisation), and through the public neighbour_list with numpy in and
+    numpy out.  Median over `calls` calls after 10 warm-up calls."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import matscipy_neighbours as m
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    rng = np.random.default_rng(0)
+    out = {}
+    for nat in sizes:
+        L = (nat / 0.08) ** (1.0 / 3.0)
+        pos = np.ascontiguousarray(rng.uniform(0.0, L, size=(nat, 3)))
+        cell = L * np.eye(3)
+        inv = np.ascontiguousarray(np.linalg.inv(cell.T))
+        pbc8 = np.ones(3, dtype=np.uint8)
+        origin = np.zeros(3)
+        pos_d = torch.from_numpy(pos).to(dev)
+        stream = torch.cuda.current_stream(dev)
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        plan = ext.plan_for(dev.index)
+        req = ext.make_request(31, origin, cell, inv, pbc8, nat, ctypes.c_void_p(pos_d.data_ptr()),
+                               True, 4.0, None, None, 0, None, dev.index)
+        n = ctypes.c_int64()
+        ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sp, ctypes.byref(n)))
+        bufs = {c: torch.empty((n.value,) + ext._SHAPES[c][0],
+                               dtype=torch.int32 if ext._SHAPES[c][1] == np.int32
+                               else torch.float64, device=dev) for c in "ijdDS"}
+        o = ext._outputs_struct(bufs, lambda t: t.data_ptr())
+
+        def abi():
+            ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sp, ctypes.byref(n)))
+            ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sp))
+            stream.synchronize()
+
+        def api():
+            m.neighbour_list("ijdDS", positions=pos, cell=cell, pbc=True, cutoff=4.0)
+
+        res = {"npairs": int(n.value)}
+        for name, f in (("c_abi_device_us", abi), ("python_api_host_us", api)):
+            ts = []
+            for k in range(calls + 10):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                f()
+                if k >= 10:
+                    ts.append(time.perf_counter() - t0)
+            res[name] = round(1e6 * statistics.median(ts), 1)
+        out[str(nat)] = res
+    return out
+
+
 def workload_config(nat, reps, npairs, world):
     """The `config` object of both arms' JSON lines (identical on purpose)."""
     return dict(WORKLOAD, natoms=nat, reps=reps, npairs_per_step=npairs,
@@ -1006,6 +1063,8 @@ def main():
                           ("C5_diff_lattice", "C5")):
             if "parity" in out["configs"].get(name, {}):
                 parity[key] = out["configs"][name]["parity"]
+    if world == 1 and not args.no_configs:
+        out["per_call_latency"] = per_call_latency(dev)
     if world == 1 and not args.no_cpu_baseline and args.reps == 64:
         want = None
         if not args.no_parity:

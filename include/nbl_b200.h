@@ -179,7 +179,7 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
                                           (one system, dense grid of at most
                                           16,384 cells) run the whole count
                                           phase as one single-CTA launch:
-                                          0 = 256, -1 = never, 1..2048
+                                          0 = 128, -1 = never, 1..2048
    No reference counterpart (the reference has no tuner). */
 typedef struct nbl_launch_config {
     int count_ctas_per_sm;

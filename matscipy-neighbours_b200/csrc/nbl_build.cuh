@@ -153,7 +153,8 @@ cudaError_t launch_lj_energy(const double *atom_e, int64_t n, double *scratch, d
 // Dense grid, one system, 1..kSmallMaxAtoms atoms (by default systems of up
 // to kSmallDefaultAtoms take it), at most kSmallMaxCells cells, every row.
 constexpr int kSmallMaxAtoms = 2048;
-constexpr int kSmallDefaultAtoms = 256;
+constexpr int kSmallDefaultAtoms = 128;
+constexpr int kSmallTile = 8;  // atoms per work item on this path at most
 constexpr int64_t kSmallMaxCells = 16384;
 struct SmallCountArgs {
     BinArgs bin;          // keys / vals: sorted in place

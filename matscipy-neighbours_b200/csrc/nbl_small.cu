@@ -15,9 +15,12 @@
 //
 // The CTA's warps take the work items one after another, each at the latency
 // of one item, so the path pays off while the system has about as many
-// items as the CTA has warps (a few hundred atoms; the default threshold).  A
-// thread-per-atom exact count in one CTA was measured as well and lost: each
-// thread walks a few hundred candidates serially.
+// items as the CTA has warps: measured on a B200, a 100-atom system's count +
+// fill + synchronisation takes 62 us this way against 65 us for the
+// multi-kernel sequence, while at 200 atoms the sequence is already faster
+// (62 against 74 us) -- hence the 128-atom default.  A thread-per-atom exact
+// count in one CTA was measured as well and lost: each thread walks a few
+// hundred candidates serially.
 #include <cstdint>
 
 #include <cuda_runtime.h>

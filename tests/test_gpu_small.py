@@ -1,5 +1,5 @@
 """The one-CTA count phase of small systems (nbl_small.cu; by default up to
-256 atoms, up to 2048 on request): it is taken when
+128 atoms, up to 2048 on request): it is taken when
 the system qualifies (one launch for the whole count phase), leaves the same
 buffers as the multi-kernel sequence -- the fill, the per-atom counts, the row
 offsets and the neighbour matrix that follow give the oracle's results bit
@@ -69,10 +69,10 @@ def ext():
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("n,kind", [(1, "scalar"), (2, "scalar"), (100, "scalar"),
-                                    (256, "per_atom"), (700, "per_atom"), (1500, "per_type"),
+                                    (128, "per_atom"), (700, "per_atom"), (1500, "per_type"),
                                     (2048, "scalar")])
 def test_small_system_is_one_launch_and_matches_the_oracle(oracle, ext, n, kind, precision):
-    if n > 256:  # above the default threshold: raise it to the largest allowed
+    if n > 128:  # above the default threshold: raise it to the largest allowed
         cfg = ext.LaunchConfig(single_cta_atoms=2048)
         ext.check(ext.lib.nbl_plan_set_launch_config(ext.plan_for(0), ctypes.byref(cfg)))
     w = _system(n, seed=n, kind=kind)
@@ -96,9 +96,9 @@ def test_larger_or_sparse_systems_keep_the_multi_kernel_sequence(oracle, ext):
 
 
 def test_threshold_and_off_switch(ext):
-    w = _system(200, seed=3)
+    w = _system(120, seed=3)
     plan = ext.plan_for(0)
-    for thr, expect_one in ((0, True), (200, True), (199, False), (-1, False)):
+    for thr, expect_one in ((0, True), (120, True), (119, False), (-1, False)):
         cfg = ext.LaunchConfig(single_cta_atoms=thr)
         ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
         back = ext.LaunchConfig()
@@ -114,10 +114,10 @@ def test_threshold_and_off_switch(ext):
 
 def test_counts_offsets_and_matrix_after_the_one_cta_count(oracle, ext):
     import matscipy_neighbours as m
-    w = _system(250, seed=4)
+    w = _system(125, seed=4)
     i, j, D = oracle.oracle_neighbour_list("ijD", w["cell"], w["positions"], w["cutoff"],
                                            w["pbc"])
-    deg = np.bincount(i, minlength=250)
+    deg = np.bincount(i, minlength=125)
     assert np.array_equal(np.asarray(m.coordination(positions=w["positions"], cell=w["cell"],
                                                     pbc=w["pbc"], cutoff=w["cutoff"])), deg)
     idx, dist, count = (np.asarray(x) for x in m.neighbour_matrix(
@@ -125,7 +125,7 @@ def test_counts_offsets_and_matrix_after_the_one_cta_count(oracle, ext):
         max_neighbours=int(deg.max())))
     assert np.array_equal(count, deg)
     start = np.concatenate([[0], np.cumsum(deg)])
-    for a in range(250):
+    for a in range(125):
         assert np.array_equal(idx[a, :deg[a]], j[start[a]:start[a + 1]])
         assert np.array_equal(dist[a, :deg[a]].view(np.int64),
                               D[start[a]:start[a + 1]].view(np.int64))
