@@ -175,11 +175,13 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
                                           grids join up to 8), 1 = one cell
                                           per item, 2..8 = at most that many
                                           (dense grid and FP32 filter only)
-     single_cta_atoms                     systems of up to this many atoms
+     one_launch_atoms                     systems of up to this many atoms
                                           (one system, dense grid of at most
                                           16,384 cells) run the whole count
-                                          phase as one single-CTA launch:
-                                          0 = 128, -1 = never, 1..2048
+                                          phase as one launch (one CTA up to
+                                          128 atoms, else a thread-block
+                                          cluster of up to 8 CTAs):
+                                          0 = the default, -1 = never, 1..2048
    No reference counterpart (the reference has no tuner). */
 typedef struct nbl_launch_config {
     int count_ctas_per_sm;
@@ -192,7 +194,7 @@ typedef struct nbl_launch_config {
     int count_large_staging;
     int atoms_per_item;
     int cells_per_item;
-    int single_cta_atoms;
+    int one_launch_atoms;
 } nbl_launch_config;
 
 NBL_API nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *cfg);

@@ -604,7 +604,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     return NBL_SUCCESS;
 }
 
-// Whether batch b takes the one-CTA count phase (nbl_small.cu): one system of
+// Whether batch b takes the one-launch count phase (nbl_small.cu): one system of
 // up to p.small_atoms atoms on a dense grid of at most kSmallMaxCells cells,
 // every row.
 static bool small_path(const Plan &p, const Batch &b) {
@@ -633,7 +633,10 @@ static nbl_status enqueue_count_small(Plan &p, const Batch &b, cudaStream_t st) 
     sa.small = B.small;
     sa.items_count = B.small + 3;
     sa.offsets = B.offsets;
-    NBL_CUDA(launch_count_small(b.fp32, p.batch_kind, sa, st), "one-CTA count phase");
+    // one CTA up to 128 atoms, else a cluster of up to 8 (about one work item
+    // per warp)
+    const int ctas = (int)std::min<int64_t>(kSmallMaxCtas, (b.natoms + 127) / 128);
+    NBL_CUDA(launch_count_small(b.fp32, p.batch_kind, sa, ctas, st), "one-launch count phase");
     return NBL_SUCCESS;
 }
 
@@ -821,7 +824,7 @@ void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
     cfg->count_large_staging = p.count_shape.cand;
     cfg->atoms_per_item = p.itile;
     cfg->cells_per_item = p.max_run;
-    cfg->single_cta_atoms = p.small_atoms == kSmallDefaultAtoms ? 0
+    cfg->one_launch_atoms = p.small_atoms == kSmallDefaultAtoms ? 0
                             : p.small_atoms > 0                ? p.small_atoms
                                                                : -1;
 }
@@ -1027,8 +1030,8 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     const int itile = cfg->atoms_per_item == 0 ? 32 : cfg->atoms_per_item;
     if (cfg->count_ctas_per_sm < 0 || cfg->count_ctas_per_sm > 64 || cfg->fill_ctas_per_sm < 0 ||
         cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 || cfg->cells_per_item < 0 ||
-        cfg->cells_per_item > kMaxRun || cfg->single_cta_atoms < -1 ||
-        cfg->single_cta_atoms > kSmallMaxAtoms || !traverse_shape_ok(kModeCount, true, cs) ||
+        cfg->cells_per_item > kMaxRun || cfg->one_launch_atoms < -1 ||
+        cfg->one_launch_atoms > kSmallMaxAtoms || !traverse_shape_ok(kModeCount, true, cs) ||
         !traverse_shape_ok(kModeFill, true, fs))
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "launch config: CTAs per SM in [0, 64], warps 2, 4 or 8, count group "
@@ -1043,9 +1046,9 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     plan->p.fill_shape = fs;
     plan->p.itile = itile;
     plan->p.max_run = cfg->cells_per_item;
-    plan->p.small_atoms = cfg->single_cta_atoms == 0   ? kSmallDefaultAtoms
-                          : cfg->single_cta_atoms < 0 ? 0
-                                                      : cfg->single_cta_atoms;
+    plan->p.small_atoms = cfg->one_launch_atoms == 0   ? kSmallDefaultAtoms
+                          : cfg->one_launch_atoms < 0 ? 0
+                                                      : cfg->one_launch_atoms;
     return NBL_SUCCESS;
 }
 

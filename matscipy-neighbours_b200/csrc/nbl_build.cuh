@@ -165,7 +165,10 @@ struct SmallCountArgs {
     int *items_count;     // == trav.n_items
     int64_t *offsets;     // [natoms + 1]
 };
-cudaError_t launch_count_small(bool fp32, int kind, const SmallCountArgs &a, cudaStream_t st);
+constexpr int kSmallMaxCtas = 8;  // a portable thread-block cluster
+// ctas: 1 (one CTA) or a thread-block cluster of up to kSmallMaxCtas CTAs.
+cudaError_t launch_count_small(bool fp32, int kind, const SmallCountArgs &a, int ctas,
+                               cudaStream_t st);
 
 // Fill the visit tables of the systems that have one (visit_base >= 0).
 cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);

@@ -32,7 +32,7 @@ def count_path(request):
     import ctypes
     from matscipy_neighbours import _matscipy_neighbours as ext
     plan = ext.plan_for(0)
-    cfg = ext.LaunchConfig(single_cta_atoms=2048 if request.param == "one_cta" else -1)
+    cfg = ext.LaunchConfig(one_launch_atoms=2048 if request.param == "one_cta" else -1)
     ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
     yield request.param
     ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(ext.LaunchConfig())))

@@ -1,5 +1,5 @@
-"""The one-CTA count phase of small systems (nbl_small.cu; by default up to
-128 atoms, up to 2048 on request): it is taken when
+"""The one-launch count phase of small systems (nbl_small.cu; by default up to
+128 atoms in one CTA, up to 2048 on request in a cluster of CTAs): it is taken when
 the system qualifies (one launch for the whole count phase), leaves the same
 buffers as the multi-kernel sequence -- the fill, the per-atom counts, the row
 offsets and the neighbour matrix that follow give the oracle's results bit
@@ -73,7 +73,7 @@ def ext():
                                     (2048, "scalar")])
 def test_small_system_is_one_launch_and_matches_the_oracle(oracle, ext, n, kind, precision):
     if n > 128:  # above the default threshold: raise it to the largest allowed
-        cfg = ext.LaunchConfig(single_cta_atoms=2048)
+        cfg = ext.LaunchConfig(one_launch_atoms=2048)
         ext.check(ext.lib.nbl_plan_set_launch_config(ext.plan_for(0), ctypes.byref(cfg)))
     w = _system(n, seed=n, kind=kind)
     launches, got = _launches_of_call(ext, w, precision)
@@ -84,7 +84,7 @@ def test_small_system_is_one_launch_and_matches_the_oracle(oracle, ext, n, kind,
 
 
 def test_larger_or_sparse_systems_keep_the_multi_kernel_sequence(oracle, ext):
-    cfg = ext.LaunchConfig(single_cta_atoms=2048)
+    cfg = ext.LaunchConfig(one_launch_atoms=2048)
     ext.check(ext.lib.nbl_plan_set_launch_config(ext.plan_for(0), ctypes.byref(cfg)))
     for w in (_system(2049, seed=1),                          # too many atoms
               _system(200, seed=2, box=120.0, pbc=(True, True, False))):  # > 16,384 cells
@@ -99,15 +99,15 @@ def test_threshold_and_off_switch(ext):
     w = _system(120, seed=3)
     plan = ext.plan_for(0)
     for thr, expect_one in ((0, True), (120, True), (119, False), (-1, False)):
-        cfg = ext.LaunchConfig(single_cta_atoms=thr)
+        cfg = ext.LaunchConfig(one_launch_atoms=thr)
         ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
         back = ext.LaunchConfig()
         ext.check(ext.lib.nbl_plan_get_launch_config(plan, ctypes.byref(back)))
-        assert back.single_cta_atoms == thr
+        assert back.one_launch_atoms == thr
         launches, _ = _launches_of_call(ext, w, "fp32")
         assert (launches == 2) == expect_one, thr
     for bad in (-2, 2049):
-        cfg = ext.LaunchConfig(single_cta_atoms=bad)
+        cfg = ext.LaunchConfig(one_launch_atoms=bad)
         assert ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)) == \
             ext.NBL_ERROR_INVALID_ARGUMENT
 
