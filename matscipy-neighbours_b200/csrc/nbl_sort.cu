@@ -165,8 +165,12 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortIters = 16;                               // per warp
-constexpr int kSortTile = kSortThreads * kSortIters;         // 4096
+// Tiles of 1024 keys: small and mid-sized inputs get enough CTAs to fill the
+// GPU (measured on a B200: count phase of 131,072 atoms 0.159 -> 0.146 ms,
+// of 16,384 atoms 0.108 -> 0.095 ms against 4096-key tiles; 1M atoms
+// unchanged).
+constexpr int kSortIters = 4;                                // per warp
+constexpr int kSortTile = kSortThreads * kSortIters;         // 1024
 constexpr int kDigitMax = 10;                 // bits per pass (at most)
 constexpr int kRadix = 1 << kDigitMax;        // bins of the widest pass
 
