@@ -1,17 +1,22 @@
 // nbl_build.cu -- the neighbour-list kernels for sm_100a.
 //
-// Pipeline (one launch sequence per batch of systems, all on one stream):
+// Pipeline (one launch sequence per batch of systems, all on one stream; the
+// per-atom and per-cell bodies of the first stages are in nbl_stages.cuh):
+//   k_init      flag block, cell table, per-system maxima, hash slots, and the
+//               visited cell offsets' vectors (reference order) per system
 //   k_bin       per atom: raw cell (reference arithmetic), fold, cell key;
 //               hashed grid: insert the cell into the open-addressing table
 //   radix sort  (nbl_sort.cu) stable by cell key -> cell-sorted atom order
 //   k_gather    per sorted atom: bin-relative position (FP64, reference
 //               arithmetic), its FP32 copy, image indices, cell slices,
 //               occupied-cell work list
-//   k_tiles     occupied cells -> work items (home cell x i-tile of <= 32 atoms)
-//   k_visit     per system: the visited cell offsets' vectors (reference order)
+//   k_tiles     occupied cells -> work items (home cell x i-tile of <= 32
+//               atoms, or runs of sparse cells along x)
 //   k_count     per work item: neighbour counts per atom, hit words
 //   scan        (nbl_sort.cu) counts -> row offsets, total pair count
 //   k_fill      per work item: writes i, j, D, d, S (or feeds a force sink)
+// A small system's count phase (init to scan) can instead be one launch
+// (nbl_small.cu).
 //
 // The traversal reproduces neighbour_visit.hh:51-120 exactly: the same
 // visited offsets in the same z/y/x order, the same cell slices in ascending
@@ -94,12 +99,10 @@ cudaError_t launch_tiles(const HomeCell *home, const int *n_home, const int2 *ta
 }
 
 
-// One block per system with a visit table: its visited offsets in the
-// traversal's z/y/x order (neighbour_visit.hh:63-84).
-__global__ void k_visit(const SysDev *__restrict__ sys, VisitDev *__restrict__ visit) {
-    visit_fill(sys[blockIdx.x], visit, threadIdx.x, blockDim.x);
-}
-
+// Start of a count phase: block s < nsys also fills system s's visit table
+// (its visited offsets in the traversal's z/y/x order, neighbour_visit.hh:
+// 63-84); every thread clears its share of the flags, the cell table (and
+// the hash slots) and the per-system maxima.
 __global__ void __launch_bounds__(256)
 k_init(const SysDev *__restrict__ sys, int nsys, VisitDev *__restrict__ visit,
        int *__restrict__ small, int2 *__restrict__ table, int64_t ntable,
@@ -128,12 +131,6 @@ cudaError_t launch_init(const SysDev *sys, int nsys, VisitDev *visit, int *small
     return cudaGetLastError();
 }
 
-cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st) {
-    if (nsys <= 0 || visit == nullptr) return cudaSuccess;
-    k_visit<<<nsys, 64, 0, st>>>(sys, visit);
-    count_launch();
-    return cudaGetLastError();
-}
 
 // Fixed-order sum of n values: block b sums values [2048 b, 2048 b + 2048)
 // (thread t: 8 consecutive values, then a fixed tree) into part2[b]; one

@@ -170,8 +170,6 @@ constexpr int kSmallMaxCtas = 8;  // a portable thread-block cluster
 cudaError_t launch_count_small(bool fp32, int kind, const SmallCountArgs &a, int ctas,
                                cudaStream_t st);
 
-// Fill the visit tables of the systems that have one (visit_base >= 0).
-cudaError_t launch_visit(const SysDev *sys, int nsys, VisitDev *visit, cudaStream_t st);
 // Start of a count phase in one launch: zero the 8-int flag block, the cell
 // table (ntable int2) and the per-system maxima, mark every hash slot empty
 // (hkey != NULL), and fill the systems' visit tables (visit != NULL).

@@ -93,7 +93,7 @@ struct SysDev {
 
 // One visited neighbour offset of a system (neighbour_visit.hh:63-84): the
 // cell offset, the offset vector in FP64 (the reference's operation order)
-// and its FP32 rounding, computed once per call by k_visit.
+// and its FP32 rounding, computed once per call by the count phase's init.
 struct VisitDev {
     double off[3];
     float off32[3];

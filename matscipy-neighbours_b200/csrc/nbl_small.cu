@@ -1,4 +1,4 @@
-// nbl_small.cu -- the whole count phase of one small system in one CTA.
+// nbl_small.cu -- the whole count phase of one small system in one launch.
 //
 // For a system of about a hundred atoms the count phase's own work is a few
 // microseconds; its cost is the chain of launches (init, bin, the sort's
