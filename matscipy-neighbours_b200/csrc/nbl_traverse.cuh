@@ -37,6 +37,12 @@ namespace {
 // table), the wrap counts and the cell slice, and a warp scan turns slice
 // lengths into candidate positions (the "segment batch").
 //
+// A run (WorkItem::run > 1, the RUN instantiations) is an item of several
+// home cells along x: its segments are the run's rows of neighbour cells,
+// each atom keeps only the segments within one cell of its own (its own
+// 3 x 3 x 3 block, in order), and D is formed with the offset of the atom's
+// own cell offset, so every row is exactly the one-cell item's row.
+//
 // k_count stages the candidates in shared memory as FP32 positions in the
 // home-cell frame (lane = segment: each copies its cell's run of sorted
 // atoms) and sweeps them against the tile's atoms, GROUP atoms per pass
@@ -52,8 +58,9 @@ namespace {
 // searches: binary search over the prefix, then an n-th-set-bit search).  The pair (exact FP64
 // D, d and S) goes to row_start + rank, so consecutive lanes write
 // consecutive slots; the next round's j-side loads are issued before this
-// round's stores.  Items without pool words (pool full, more than one segment
-// batch) recompute the words with the count's sweep first.
+// round's stores.  Items without pool words (pool full, more than
+// kMaskBatches segment batches) recompute the words with the count's sweep
+// first.
 namespace {
 
 constexpr int kSeg = 32;         // visited offsets per batch (one per lane)
