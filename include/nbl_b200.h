@@ -182,6 +182,17 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
                                           128 atoms, else a thread-block
                                           cluster of up to 8 CTAs):
                                           0 = the default, -1 = never, 1..2048
+     thread_per_atom                      pair passes with one thread per atom
+                                          instead of one warp per work item:
+                                          0 = where the occupied cells hold
+                                          fewer than two atoms on average
+                                          (known after a first count of the
+                                          same sizes; before it, fewer atoms
+                                          than cells), -1 =
+                                          never, 1 = always (systems with a
+                                          visit table: at most 2^20 visited
+                                          offsets in all); the force sink
+                                          always uses work items
    No reference counterpart (the reference has no tuner). */
 typedef struct nbl_launch_config {
     int count_ctas_per_sm;
@@ -195,6 +206,7 @@ typedef struct nbl_launch_config {
     int atoms_per_item;
     int cells_per_item;
     int one_launch_atoms;
+    int thread_per_atom;
 } nbl_launch_config;
 
 NBL_API nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *cfg);

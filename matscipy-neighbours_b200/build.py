@@ -35,7 +35,7 @@ SOURCES = ["nbl_api.cu", "nbl_build.cu", "nbl_sort.cu", "nbl_noalloc.cu",
            "nbl_batch.cu", "nbl_backward.cu", "nbl_csr.cu", "nbl_verlet.cu",
            "nbl_trav_count32.cu", "nbl_trav_count32r.cu", "nbl_trav_count64.cu",
            "nbl_trav_fill32.cu", "nbl_trav_fill32r.cu", "nbl_trav_fill64.cu",
-           "nbl_small.cu"]
+           "nbl_small.cu", "nbl_trav_atoms.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", f"-I{INCLUDE}", f"-I{CSRC}",

@@ -406,6 +406,25 @@ static int run_limit(const Plan &p, const Batch &b) {
     return p.max_run;
 }
 
+// Whether the pair passes run one thread per atom (nbl_trav_atoms.cu) for
+// batch b: every system needs its visit table; by default only where the
+// occupied cells hold fewer than two atoms on average, so that a warp's work
+// item would hold one or two atoms.  The occupied cells are known once a
+// count of the same sizes has run on the plan; before that, fewer atoms than
+// cells stands in for it.  Measured on 200,000-atom uniform gases (count +
+// fill): 2.7x faster at 0.25 atoms per cell (1.1 per occupied cell), 2.0x at
+// 0.5 (1.3), 1.35x at 1 (1.6), even at 2 (2.3), slower above; even on a slab
+// of 2 atoms per occupied cell.  The force sink always takes the work items.
+static bool atom_mode(const Plan &p, const Batch &b) {
+    if (p.no_atoms || p.atom_threads < 0 || p.bufs.visit == nullptr) return false;
+    if (p.atom_threads > 0) return true;
+    if (p.occ_cells > 0 && p.occ_natoms == b.natoms && p.occ_table == b.table_size)
+        return (double)b.natoms < 2.0 * (double)p.occ_cells;
+    double cells = 0.0;
+    for (int64_t n : b.ncells) cells += (double)n;
+    return (double)b.natoms < cells;
+}
+
 // Size the workspace for a batch and copy its inputs and host tables in.
 nbl_status upload_batch(Plan &p, const Batch &b, cudaStream_t st) {
     nbl_status s = layout_workspace(p, b);
@@ -546,6 +565,9 @@ static void traverse_args(Plan &p, const Batch &b) {
     ta.itile = p.itile;
     ta.natoms = N;
     ta.runs = run_limit(p, b) != 1 ? 1 : 0;
+    ta.atoms = atom_mode(p, b) ? 1 : 0;
+    ta.sys_atom_base = B.sys_atom_base;
+    ta.nsys = (int)b.sys.size();
     p.batch_kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
     p.trav_grid = traverse_grid(p, N, p.count_mult, kModeCount, b.fp32, p.batch_kind,
                                 p.count_shape, false);
@@ -579,14 +601,17 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
     }
     GatherArgs ga;
     gather_args(p, b, in_alt ? B.keys2 : B.keys, in_alt ? B.vals2 : B.vals, ga);
+    const bool atoms = atom_mode(p, b);
     {
         StageRange r("nbl.gather");
         NBL_CUDA(launch_gather(ga, st), "k_gather");
-        NBL_CUDA(launch_tiles(B.home, ga.n_home, B.table, B.sys, B.items, B.small + 3, N,
-                              p.num_sms, p.itile, run_limit(p, b), st),
-                 "k_tiles");
+        if (!atoms)  // the thread-per-atom passes need no work items
+            NBL_CUDA(launch_tiles(B.home, ga.n_home, B.table, B.sys, B.items, B.small + 3, N,
+                                  p.num_sms, p.itile, run_limit(p, b), st),
+                     "k_tiles");
     }
     traverse_args(p, b);
+    p.targs.skeys = in_alt ? B.keys2 : B.keys;
     if (p.i_lo > 0 || p.i_hi < N)
         NBL_CUDA(cudaMemsetAsync(B.counts, 0, sizeof(int32_t) * N, st), "memset counts");
     {
@@ -623,6 +648,7 @@ static nbl_status enqueue_count_small(Plan &p, const Batch &b, cudaStream_t st) 
     bin_args(p, b, sa.bin);
     gather_args(p, b, B.keys, B.vals, sa.gather);
     traverse_args(p, b);
+    p.targs.atoms = 0;  // the one-launch count builds work items for the warp passes
     // Work items of at most 8 atoms: a small system's passes are bound by the
     // latency of one item, which shrinks with its tile (100 atoms: 74 -> 62 us
     // for count + fill + synchronisation against 32-atom items).
@@ -671,6 +697,7 @@ static CountKey count_key(const Plan &p, const Batch &b) {
     k.count_cand = p.count_shape.cand;
     k.count_group = p.count_shape.group;
     k.count_tickets = p.count_tickets ? 1 : 0;
+    k.atoms = atom_mode(p, b) ? 1 : 0;
     return k;
 }
 
@@ -760,6 +787,11 @@ nbl_status run_count(Plan &p, const Batch &b, cudaStream_t st, bool sync) {
         int flags[6];
         std::memcpy(flags, p.host_small + 1, sizeof(flags));
         p.npairs = p.host_small[0];
+        if (flags[0] > 0) {  // occupied cells, for the next call's choice of passes
+            p.occ_natoms = N;
+            p.occ_table = b.table_size;
+            p.occ_cells = flags[0];
+        }
         unsigned long long demand = 0;  // mask-pool words the count asked for
         std::memcpy(&demand, flags + 4, sizeof(demand));
         p.mask_hint = (int64_t)demand;
@@ -827,6 +859,7 @@ void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
     cfg->one_launch_atoms = p.small_atoms == kSmallDefaultAtoms ? 0
                             : p.small_atoms > 0                ? p.small_atoms
                                                                : -1;
+    cfg->thread_per_atom = p.atom_threads;
 }
 
 // Request -> one-system batch.
@@ -1032,12 +1065,13 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
         cfg->fill_ctas_per_sm > 64 || itile < 1 || itile > 32 || cfg->cells_per_item < 0 ||
         cfg->cells_per_item > kMaxRun || cfg->one_launch_atoms < -1 ||
         cfg->one_launch_atoms > kSmallMaxAtoms || !traverse_shape_ok(kModeCount, true, cs) ||
-        !traverse_shape_ok(kModeFill, true, fs))
+        !traverse_shape_ok(kModeFill, true, fs) || cfg->thread_per_atom < -1 ||
+        cfg->thread_per_atom > 1)
         return set_error(NBL_ERROR_INVALID_ARGUMENT,
                          "launch config: CTAs per SM in [0, 64], warps 2, 4 or 8, count group "
                          "2 or 4, large candidate staging 0 or 1, atoms per item in [1, 32], "
-                         "cells per item in [0, %d], single-CTA atoms in [-1, %d]", kMaxRun,
-                         kSmallMaxAtoms);
+                         "cells per item in [0, %d], single-CTA atoms in [-1, %d], thread per "
+                         "atom -1, 0 or 1", kMaxRun, kSmallMaxAtoms);
     plan->p.count_mult = cfg->count_ctas_per_sm;
     plan->p.fill_mult = cfg->fill_ctas_per_sm;
     plan->p.count_tickets = cfg->count_strided == 0;
@@ -1049,6 +1083,7 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     plan->p.small_atoms = cfg->one_launch_atoms == 0   ? kSmallDefaultAtoms
                           : cfg->one_launch_atoms < 0 ? 0
                                                       : cfg->one_launch_atoms;
+    plan->p.atom_threads = cfg->thread_per_atom;
     return NBL_SUCCESS;
 }
 
@@ -1214,7 +1249,9 @@ nbl_status nbl_lj_forces(nbl_plan *plan, const nbl_request *req, double epsilon,
     if (!g.ok) return set_error(NBL_ERROR_CUDA, "cannot select device %d", plan->p.device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     Plan &p = plan->p;
+    p.no_atoms = true;  // the force sink takes the work items
     st = run_count(p, b, cs, false);
+    p.no_atoms = false;
     if (st != NBL_SUCCESS) return st;
     if (b.natoms == 0) {
         NBL_CUDA(cudaMemsetAsync(energy, 0, sizeof(double), cs), "memset energy");

@@ -232,6 +232,11 @@ cudaError_t launch_traverse(int mode, bool fp32, int kind, const TraverseArgs &a
                             int grid, cudaStream_t st, const TravShape &shape) {
     if (grid <= 0) return cudaSuccess;
     if (!traverse_shape_ok(mode, fp32, shape)) return cudaErrorInvalidValue;
+    if (a.atoms) {  // one thread per atom; precision does not apply (exact FP64)
+        if (a.lj_force != nullptr) return cudaErrorInvalidValue;
+        return mode == kModeCount ? launch_count_atoms(kind, a, st)
+                                  : launch_fill_atoms(kind, a, st);
+    }
     if (!fp32) {
         return mode == kModeCount ? launch_count_fp64(kind, a, grid, st, shape)
                                   : launch_fill_fp64(kind, a, grid, st, shape);

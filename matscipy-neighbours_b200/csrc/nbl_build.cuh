@@ -114,6 +114,14 @@ struct TraverseArgs {
     // Nonzero: k_tiles may have joined home cells into runs (WorkItem::run),
     // so the pair passes use the instantiations that take them.
     int runs;
+    // Nonzero: the pair passes run one thread per sorted atom
+    // (nbl_trav_atoms.cu) instead of one warp per work item; no work items
+    // or hit words are built.  Needs the sorted cell keys, the systems'
+    // atom bases and the visit tables.
+    int atoms;
+    const uint32_t *skeys;          // sorted cell keys (the sort's output)
+    const int64_t *sys_atom_base;   // first atom of each system
+    int nsys;
 };
 
 // Launch shape of one pair pass: warps per CTA (2, 4 or 8, i.e. 64, 128 or
@@ -215,6 +223,11 @@ cudaError_t launch_fill_fp32_runs(int kind, const TraverseArgs &a, int grid, cud
 int occupancy_count_fp32_runs(int kind, const TravShape &shape);
 int occupancy_fill_fp32_runs(int kind, const TravShape &shape, bool lj);
 int occupancy_count_fp64(int kind, const TravShape &shape);
+// The thread-per-atom passes (TraverseArgs::atoms, nbl_trav_atoms.cu): one
+// thread per sorted atom walks its visited cells in the reference's order
+// with the exact FP64 test; the grid covers the atoms.  No force sink.
+cudaError_t launch_count_atoms(int kind, const TraverseArgs &a, cudaStream_t st);
+cudaError_t launch_fill_atoms(int kind, const TraverseArgs &a, cudaStream_t st);
 int occupancy_fill_fp32(int kind, const TravShape &shape, bool lj);
 int occupancy_fill_fp64(int kind, const TravShape &shape, bool lj);
 

@@ -91,7 +91,7 @@ struct CountKey {
     const void *ws_base, *pos, *per_atom, *types;
     int64_t natoms, table_size, mask_cap, pt_size, i_lo, i_hi;
     int32_t nsys, grid, key_bits, fp32, kind, itile, max_run, nvisit_tab;
-    int32_t count_mult, count_warps, count_cand, count_group, count_tickets;
+    int32_t count_mult, count_warps, count_cand, count_group, count_tickets, atoms;
     CountKey() { std::memset(this, 0, sizeof(*this)); }
     bool operator==(const CountKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -121,6 +121,15 @@ struct Plan {
     // Systems of up to this many atoms (at most kSmallMaxAtoms) take the
     // one-CTA count phase; 0: never.
     int small_atoms = kSmallDefaultAtoms;
+    // Pair passes with one thread per atom (nbl_trav_atoms.cu): 0 = where the
+    // occupied cells hold fewer than two atoms on average, -1 = never, 1 =
+    // always (where the systems have visit tables).  no_atoms turns them off
+    // for one count (the force sink needs the work items).
+    int atom_threads = 0;
+    bool no_atoms = false;
+    // Occupied cells counted by the last synchronised count, with the atom
+    // count and table size it ran on (steers the default choice above).
+    int64_t occ_natoms = -1, occ_table = -1, occ_cells = 0;
     // Work items by atomic ticket (else a fixed warp stride) in each pass.
     bool count_tickets = true;
     bool fill_tickets = true;

@@ -81,7 +81,7 @@ class LaunchConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "count_ctas_per_sm", "fill_ctas_per_sm", "count_strided", "fill_strided",
         "count_warps", "fill_warps", "count_group", "count_large_staging",
-        "atoms_per_item", "cells_per_item", "one_launch_atoms")]
+        "atoms_per_item", "cells_per_item", "one_launch_atoms", "thread_per_atom")]
 
     def as_dict(self):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}

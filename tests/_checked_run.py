@@ -3,8 +3,8 @@ path, compared with the CPU oracle.  Run as a child process by
 test_gpu_checked.py with MATSCIPY_NEIGHBOURS_CHECKED=1, because the library
 is chosen once per process when the package is imported.
 
-The checked build tests, inside the pair passes, every cell slice, candidate
-index, hit-word index and output slot (the slot must lie in its own row
+The checked build tests, inside the pair passes (warp and thread-per-atom),
+every cell slice, candidate index, hit-word index and output slot (the slot must lie in its own row
 [offsets[i], offsets[i+1])); a failed test would come back as
 NBL_ERROR_INTERNAL ("device-side bound exceeded").  So a clean run here shows
 that none of those indices leaves its bounds on these inputs, and the oracle
@@ -175,6 +175,30 @@ def matrix_and_forces():
     DONE[0] += 1
 
 
+def thread_per_atom():
+    """The thread-per-atom pair passes over the golden cases (every grid) and
+    the workload shapes."""
+    plan = ext.plan_for(0)
+    cfg = ext.LaunchConfig(thread_per_atom=1, one_launch_atoms=-1)
+    ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
+    try:
+        for case in golden_cases():
+            if case["npairs"] > 2_000_000:
+                continue
+            for grid in ("dense", "morton", "hashed"):
+                out = _device_list(case["quantities"], case, "fp32", grid)
+                for q, a in zip(case["quantities"], out):
+                    assert digest(a) == case["digest"][q], (case["name"], q, grid)
+                DONE[0] += 1
+        for w in (W.sparse_slab(n=20000), W.fcc_bulk(reps=6)):
+            want = _want("ijdDS", w)
+            assert_same_lists(_device_list("ijdDS", w), want, "ijdDS")
+            assert_same_lists(_device_list("ijd", w), want[:3], "ijd")
+            DONE[0] += 2
+    finally:
+        ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(ext.LaunchConfig())))
+
+
 def main():
     assert ext.CHECKED and ext._LIB_PATH.name == "libnbl_b200_checked.so"
     torch.cuda.set_device(0)
@@ -184,6 +208,7 @@ def main():
     row_slices()
     batch()
     matrix_and_forces()
+    thread_per_atom()
     libs = _loaded_libraries()
     assert libs == {"libnbl_b200_checked.so"}, libs
     print(f"checked ok {DONE[0]}")

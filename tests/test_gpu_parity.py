@@ -1,8 +1,10 @@
 """GPU engine vs the CPU oracle: bit-identical outputs (same arrays, same
 order) for every precision mode and grid layout, on the reference's golden
 cases, the five workload shapes at reduced size, and edge cases.  The golden
-and edge cases run through both count phases: the one-CTA launch that small
-systems take by default and the multi-kernel sequence (single-CTA path off)."""
+and edge cases run through three count paths: the one-CTA launch that small
+systems take by default, the multi-kernel sequence with warp work items
+(single-CTA path off) and the multi-kernel sequence with the thread-per-atom
+pair passes."""
 import itertools
 
 import numpy as np
@@ -25,14 +27,16 @@ def _restore_options():
     set_options(precision=prev["precision"], grid=prev["grid"])
 
 
-@pytest.fixture(params=["one_cta", "multi_kernel"])
+@pytest.fixture(params=["one_cta", "multi_kernel", "thread_per_atom"])
 def count_path(request):
     """The plan's single-CTA threshold: its largest value (every golden and
-    edge case that fits takes the one-CTA count phase), or -1 (never)."""
+    edge case that fits takes the one-CTA count phase), or -1 (never); and
+    the multi-kernel sequence with the thread-per-atom pair passes forced on."""
     import ctypes
     from matscipy_neighbours import _matscipy_neighbours as ext
     plan = ext.plan_for(0)
-    cfg = ext.LaunchConfig(one_launch_atoms=2048 if request.param == "one_cta" else -1)
+    cfg = ext.LaunchConfig(one_launch_atoms=2048 if request.param == "one_cta" else -1,
+                           thread_per_atom=1 if request.param == "thread_per_atom" else -1)
     ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
     yield request.param
     ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(ext.LaunchConfig())))
