@@ -319,14 +319,18 @@ def batched_bench(steps, warmup, dev, rank=0, check=False):
     return out
 
 
-def configs_bench(dev, flush, reps=10, only=None, check=False):
+def configs_bench(dev, flush, reps=10, only=None, check=False, thread_per_atom=0):
     """The other configurations beside the headline (rank 0, N = 1): C1 plain
-    small, C3 sparse slab (per-type cutoffs, ijdD), C5 differentiation lattice.
-    Each: positions resident on the device, median of `reps` full builds
-    (count + fill) by CUDA events with the L2 flushed before each, and the
-    reference's CPU core on the same input (all host threads, median of 3).
+    small, C3 sparse slab (per-type cutoffs, ijdD), C5 differentiation lattice,
+    and a dilute gas (200,000 atoms, 0.5 per cell).  Each: positions resident
+    on the device, median of `reps` full builds (count + fill) by CUDA events
+    with the L2 flushed before each, and the reference's CPU core on the same
+    input (all host threads, median of 3).  C3 and the dilute gas also time
+    both pair-pass forms (one warp per work item, one thread per atom).
     C5 adds the backward kernel (nbl_backward, gradients of D and d), timed
-    alone, with its HBM roofline: npairs * 84 + nat * 48 algorithmic bytes."""
+    alone, with its HBM roofline: npairs * 84 + nat * 48 algorithmic bytes.
+    `thread_per_atom` is the plans' launch-config setting for every line
+    (0: the default choice, 1: on, -1: off)."""
     import ctypes
 
     import numpy as np
@@ -350,9 +354,15 @@ def configs_bench(dev, flush, reps=10, only=None, check=False):
     def wanted(name):
         return only is None or name in only
 
+    def set_passes(setting):
+        cfg = ext.LaunchConfig(thread_per_atom=setting)
+        ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(cfg)))
+
+    set_passes(thread_per_atom)
     for name, make in (("C1_plain_small", W.plain_small),
                        ("C3_sparse_slab", W.sparse_slab),
-                       ("C5_diff_lattice", W.diff_lattice)):
+                       ("C5_diff_lattice", W.diff_lattice),
+                       ("gas_dilute", W.dilute_gas)):
         if not wanted(name):
             continue
         w = make()
@@ -407,6 +417,33 @@ def configs_bench(dev, flush, reps=10, only=None, check=False):
             grid_rows[grid] = (statistics.median(ms), statistics.median(cms),
                                statistics.median(fms))
         gpu_ms, count_ms, fill_ms = grid_rows["auto"]
+        passes = {}
+        if name.startswith(("C3", "gas")):
+            # both pair-pass forms on the same input (auto grid)
+            prev = ext.set_options(grid="auto")
+            req = ext.make_request(flags, origin, cell, inv, pbc8, nat,
+                                   ctypes.c_void_p(pos.data_ptr()), True, rc, pa, pt, nc,
+                                   types, dev.index)
+            ext.set_options(grid=prev["grid"])
+            for form, setting in (("warp_per_item", -1), ("thread_per_atom", 1)):
+                set_passes(setting)
+                ms = []
+                for k in range(reps + 3):
+                    flush.zero_()
+                    torch.cuda.synchronize(dev)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e2 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ext.check(ext.lib.nbl_count(plan, ctypes.byref(req), sptr,
+                                                ctypes.byref(n)))
+                    ext.check(ext.lib.nbl_fill(plan, ctypes.byref(o), sptr))
+                    e2.record(stream)
+                    e2.synchronize()
+                    if k >= 3:
+                        ms.append(e0.elapsed_time(e2))
+                ext.check(ext.lib.nbl_check(plan, sptr))
+                passes[form] = statistics.median(ms)
+            set_passes(thread_per_atom)
         gpu_s = gpu_ms * 1e-3
         cpu_args = (q, w["cell"], w["positions"], w["cutoff"], w["pbc"])
         cpu_fn(*cpu_args, types=types)
@@ -433,6 +470,8 @@ def configs_bench(dev, flush, reps=10, only=None, check=False):
                "speedup": cpu_s / gpu_s}
         if len(grids) > 1:
             row["grids_ms"] = {g: v[0] for g, v in grid_rows.items()}
+        if passes:
+            row["pair_passes_ms"] = passes
         if check:
             # the bufs hold the last grid's build; every grid gives the same list
             row["parity"] = _same_device(q, [bufs[c] for c in q], res)
@@ -868,6 +907,9 @@ def main():
     ap.add_argument("--only-configs", default=None,
                     help="comma-separated config lines to run alone (e.g. C5_diff_lattice, "
                          "LJ_droplet_1M, verlet_C2); prints them and nothing else")
+    ap.add_argument("--thread-per-atom", default="auto", choices=["auto", "on", "off"],
+                    help="pair passes of the C1/C3/C5/dilute-gas lines: the default "
+                         "choice, one thread per atom, or one warp per work item")
     ap.add_argument("--reps", type=int, default=64,
                     help="FCC unit cells per edge (64 = the benchmark size; smaller "
                          "values make the small cases used for profiling)")
@@ -895,7 +937,9 @@ def main():
     if args.only_configs:
         flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
         only = set(x.strip() for x in args.only_configs.split(",") if x.strip())
-        print(json.dumps({"configs": configs_bench(dev, flush, only=only)}), flush=True)
+        tpa = {"auto": 0, "on": 1, "off": -1}[args.thread_per_atom]
+        print(json.dumps({"configs": configs_bench(dev, flush, only=only,
+                                                   thread_per_atom=tpa)}), flush=True)
         return
     dist = None
     if world > 1:
@@ -1058,9 +1102,11 @@ def main():
         if "parity" in out["batched"]:
             parity["C4"] = out["batched"]["parity"]
     if world == 1 and not args.no_configs:
-        out["configs"] = configs_bench(dev, flush, check=not args.no_parity)
+        out["configs"] = configs_bench(dev, flush, check=not args.no_parity,
+                                       thread_per_atom={"auto": 0, "on": 1,
+                                                        "off": -1}[args.thread_per_atom])
         for name, key in (("C1_plain_small", "C1"), ("C3_sparse_slab", "C3"),
-                          ("C5_diff_lattice", "C5")):
+                          ("C5_diff_lattice", "C5"), ("gas_dilute", "gas_dilute")):
             if "parity" in out["configs"].get(name, {}):
                 parity[key] = out["configs"][name]["parity"]
     if world == 1 and not args.no_configs:

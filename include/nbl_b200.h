@@ -167,7 +167,10 @@ NBL_API nbl_status nbl_plan_set_launch(nbl_plan *plan, int count_ctas_per_sm, in
                                           0 = 384 (FP32) / 192 (FP64),
                                           1 = 768 / 384
      atoms_per_item                       cell-occupancy tile: atoms of one
-                                          cell per work item, 1..32 (32)
+                                          cell per work item, 1..32; 0 = by
+                                          the atom count: 4 up to 4,096
+                                          atoms, 8 up to 16,384, 16 up to
+                                          65,536, else 32
      cells_per_item                       home cells one work item may join
                                           along x when their atoms fit one
                                           tile: 0 = chosen on the device from

@@ -406,6 +406,23 @@ static int run_limit(const Plan &p, const Batch &b) {
     return p.max_run;
 }
 
+// Atoms per work item (the cell-occupancy tile) for batch b: the launch
+// configuration's, or by default chosen from the atom count.  A small system
+// has few work items however its cells are cut, and its call time is the
+// latency of the longest item, so it is cut finer: single calls through the
+// C-ABI measured on one B200 (count + fill + synchronisation) took, at tiles
+// of 32 / 16 / 8 / 4 atoms, 122 / 99 / 86 / 79 us for 1,000 atoms (15.6 per
+// cell) and 212 / 150 / 117 / 101 us on average over 300 of the batched
+// small periodic systems (691 / 397 / 244 / 167 us with the plain FP64
+// test).  Large systems keep 32: their cells hold fewer atoms than that.
+static int tile_of(const Plan &p, const Batch &b) {
+    if (!p.itile_auto) return p.itile;
+    if (b.natoms <= 4096) return 4;
+    if (b.natoms <= 16384) return 8;
+    if (b.natoms <= 65536) return 16;
+    return p.itile;
+}
+
 // Whether the pair passes run one thread per atom (nbl_trav_atoms.cu) for
 // batch b: every system needs its visit table; by default only where the
 // occupied cells hold fewer than two atoms on average, so that a warp's work
@@ -562,7 +579,7 @@ static void traverse_args(Plan &p, const Batch &b) {
     ta.err = B.small + 1;
     ta.i_lo = p.i_lo;
     ta.i_hi = p.i_hi;
-    ta.itile = p.itile;
+    ta.itile = tile_of(p, b);
     ta.natoms = N;
     ta.runs = run_limit(p, b) != 1 ? 1 : 0;
     ta.atoms = atom_mode(p, b) ? 1 : 0;
@@ -607,7 +624,7 @@ nbl_status enqueue_count(Plan &p, const Batch &b, cudaStream_t st) {
         NBL_CUDA(launch_gather(ga, st), "k_gather");
         if (!atoms)  // the thread-per-atom passes need no work items
             NBL_CUDA(launch_tiles(B.home, ga.n_home, B.table, B.sys, B.items, B.small + 3, N,
-                                  p.num_sms, p.itile, run_limit(p, b), st),
+                                  p.num_sms, tile_of(p, b), run_limit(p, b), st),
                      "k_tiles");
     }
     traverse_args(p, b);
@@ -652,7 +669,7 @@ static nbl_status enqueue_count_small(Plan &p, const Batch &b, cudaStream_t st) 
     // Work items of at most 8 atoms: a small system's passes are bound by the
     // latency of one item, which shrinks with its tile (100 atoms: 74 -> 62 us
     // for count + fill + synchronisation against 32-atom items).
-    p.targs.itile = std::min(p.itile, kSmallTile);
+    p.targs.itile = p.itile_auto ? kSmallTile : std::min(p.itile, kSmallTile);
     sa.trav = p.targs;
     sa.trav.item_next = p.count_tickets ? B.small + 6 : nullptr;
     sa.ncells = b.table_size;
@@ -689,7 +706,7 @@ static CountKey count_key(const Plan &p, const Batch &b) {
     k.key_bits = b.key_bits;
     k.fp32 = b.fp32 ? 1 : 0;
     k.kind = b.sys.empty() ? kCutScalar : b.sys[0].cutoff_kind;
-    k.itile = p.itile;
+    k.itile = tile_of(p, b);
     k.max_run = run_limit(p, b);
     k.nvisit_tab = p.bufs.visit != nullptr ? 1 : 0;
     k.count_mult = p.count_mult;
@@ -854,7 +871,7 @@ void launch_config_of(const Plan &p, nbl_launch_config *cfg) {
     cfg->fill_warps = p.fill_shape.warps;
     cfg->count_group = p.count_shape.group;
     cfg->count_large_staging = p.count_shape.cand;
-    cfg->atoms_per_item = p.itile;
+    cfg->atoms_per_item = p.itile_auto ? 0 : p.itile;
     cfg->cells_per_item = p.max_run;
     cfg->one_launch_atoms = p.small_atoms == kSmallDefaultAtoms ? 0
                             : p.small_atoms > 0                ? p.small_atoms
@@ -1079,6 +1096,7 @@ nbl_status nbl_plan_set_launch_config(nbl_plan *plan, const nbl_launch_config *c
     plan->p.count_shape = cs;
     plan->p.fill_shape = fs;
     plan->p.itile = itile;
+    plan->p.itile_auto = cfg->atoms_per_item == 0;
     plan->p.max_run = cfg->cells_per_item;
     plan->p.small_atoms = cfg->one_launch_atoms == 0   ? kSmallDefaultAtoms
                           : cfg->one_launch_atoms < 0 ? 0

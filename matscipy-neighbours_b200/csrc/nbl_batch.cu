@@ -259,6 +259,7 @@ void apply_choice(Plan &p, const TuneChoice &c) {
     p.count_shape.group = c.count_group;
     p.fill_shape.warps = c.fill_warps;
     p.itile = c.itile;
+    p.itile_auto = false;
 }
 
 // Fill grid for `mult` CTAs per SM (the cap nbl_count's planning applies).

@@ -114,6 +114,9 @@ struct Plan {
     TravShape count_shape;
     TravShape fill_shape = default_fill_shape();
     int itile = 32;
+    // Tile chosen per call from the atom count (launch config atoms_per_item
+    // 0); itile is then the tile of large systems.
+    bool itile_auto = true;
     // Home cells per work item at most (0: chosen on the device from the
     // cells' mean occupancy; 1: one cell per item).  Runs of several cells
     // are only built on the dense grid with the FP32 filter.

@@ -55,6 +55,18 @@ def sparse_slab(seed=0, n=200_000, box=400.0, z0=180.0, z1=220.0,
                 quantities="ijdD")
 
 
+def dilute_gas(seed=0, n=200_000, per_cell=0.5, cutoff=3.0):
+    """n atoms uniform in a periodic cube sized so that the cutoff-sized cell
+    grid holds `per_cell` atoms per cell on average (0.5: about 1.3 atoms
+    per occupied cell), scalar cutoff, ijdDS."""
+    rng = np.random.default_rng(seed)
+    box = (n / per_cell) ** (1.0 / 3.0) * cutoff
+    pos = rng.uniform(0.0, box, size=(n, 3))
+    return dict(positions=pos, cell=np.diag([box, box, box]).astype(float),
+                pbc=np.array([True, True, True]), cutoff=float(cutoff),
+                quantities="ijdDS")
+
+
 def _triclinic_cell(rng, edges, angles_deg):
     a, b, c = edges
     al, be, ga = np.radians(angles_deg)
