@@ -2,7 +2,7 @@
 against the cutoff (many periodic images down to sparse grids), mixed
 periodicity, atoms outside the box, scalar / per-atom / per-type cutoffs --
 each through a random engine configuration (precision, grid layout, atoms per
-work item, runs of cells, the one-launch count phase) and compared with the
+work item, runs of cells, the one-launch count phase, the pair-pass form) and compared with the
 CPU oracle bit for bit, row order included."""
 import ctypes
 
@@ -45,7 +45,8 @@ def _case(seed):
                grid=str(rng.choice(["auto", "dense", "morton", "hashed"])),
                atoms_per_item=int(rng.choice([0, 5, 16])),
                cells_per_item=int(rng.choice([0, 1, 4, 8])),
-               one_launch_atoms=int(rng.choice([0, -1, 2048])))
+               one_launch_atoms=int(rng.choice([0, -1, 2048])),
+               thread_per_atom=int(rng.choice([0, -1, 1])))
     return dict(positions=pos, cell=cell, pbc=pbc, cutoff=cutoff, types=types), cfg
 
 
@@ -61,7 +62,8 @@ def test_random_system_and_configuration(oracle, seed):
     ext.set_options(precision=cfg["precision"], grid=cfg["grid"])
     lc = ext.LaunchConfig(atoms_per_item=cfg["atoms_per_item"],
                           cells_per_item=cfg["cells_per_item"],
-                          one_launch_atoms=cfg["one_launch_atoms"])
+                          one_launch_atoms=cfg["one_launch_atoms"],
+                          thread_per_atom=cfg["thread_per_atom"])
     ext.check(ext.lib.nbl_plan_set_launch_config(plan, ctypes.byref(lc)))
     try:
         want = oracle.oracle_neighbour_list("ijdDS", w["cell"], w["positions"], w["cutoff"],
