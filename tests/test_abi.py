@@ -75,3 +75,29 @@ def test_api_fails_loudly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError):
         m.neighbour_list("ij", positions=np.zeros((2, 3)), cell=np.eye(3), cutoff=1.0)
+
+
+def _header_struct_fields(name):
+    text = (ROOT / "include" / "nbl_b200.h").read_text()
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    return re.findall(r"\b(\w+)\s*;", body)
+
+
+def test_launch_config_layout_matches_the_header():
+    """The binding's nbl_launch_config mirror has the header's fields, in
+    order, all int (a field added on one side only would shift the others)."""
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    fields = _header_struct_fields("nbl_launch_config")
+    assert [n for n, _ in ext.LaunchConfig._fields_] == fields
+    assert all(t is ctypes.c_int for _, t in ext.LaunchConfig._fields_)
+    assert "thread_per_atom" in fields and "atoms_per_item" in fields
+
+
+def test_launch_config_needs_a_plan():
+    from matscipy_neighbours import _matscipy_neighbours as ext
+    cfg = ext.LaunchConfig(thread_per_atom=1)
+    assert ext.lib.nbl_plan_set_launch_config(None, ctypes.byref(cfg)) == \
+        ext.NBL_ERROR_INVALID_ARGUMENT
+    assert ext.lib.nbl_plan_get_launch_config(None, ctypes.byref(cfg)) == \
+        ext.NBL_ERROR_INVALID_ARGUMENT
