@@ -85,11 +85,15 @@ def test_oracle_equals_reference_core_when_built(oracle):
     if not oracle.ref_available():
         pytest.skip("reference core not compiled here")
     from matscipy_neighbours import _workloads as W
-    for w in (W.plain_small(), W.fcc_bulk(reps=10), W.diff_lattice(shape=(10, 10, 8))):
+    for w in (W.plain_small(), W.fcc_bulk(reps=10), W.diff_lattice(shape=(10, 10, 8)),
+              W.sparse_slab(n=20000), W.dilute_gas(n=20000)):
+        types = w.get("numbers")
+        types = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
         a = oracle.oracle_neighbour_list("ijdDS", w["cell"], w["positions"], w["cutoff"],
-                                         w["pbc"])
+                                         w["pbc"], types=types)
         b = oracle.ref_neighbour_list("ijdDS", w["cell"], w["positions"], w["cutoff"],
-                                      w["pbc"])
+                                      w["pbc"], types=types)
+        assert len(a[0]) > 0
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
 
